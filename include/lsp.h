@@ -1,0 +1,176 @@
+/*
+ * lsp.h -- C ABI of liquidsimulation_b200, the B200 (sm_100a) implementation of
+ * LiquidPhysics' per-step SPH / PCISPH particle pipeline.
+ *
+ * The reference exposes its solver as C++ classes (LiquidPhysics/include/SPHSolver.h,
+ * PCISPHSolver.h, PhysicSolver.h) over a device seam (Parallelization/
+ * ParallelComputationInterface.h). This header replaces both with a handle-based
+ * C ABI: plain pointers and sizes, caller-owned host buffers, solver-owned device
+ * memory. One handle = one scene = one CUDA stream; a handle is not re-entrant.
+ *
+ * Every call returns an int status: LSP_OK (0) or a negative LSP_ERR_* code.
+ * lsp_last_error() gives a message for the last failing call on this thread.
+ *
+ * Particle order: every array passed in or out is in CALLER order (the order
+ * particles were added). The device keeps particles sorted by grid cell; the
+ * library maps back, so callers never see the device order (the reference's
+ * OpenCL path instead hands back sorted data, SPHSolver.cpp:412-422).
+ */
+#ifndef LSP_H
+#define LSP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LSP_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define LSP_OK                   0
+#define LSP_ERR_INVALID         -1   /* bad argument (null pointer, size, value out of range) */
+#define LSP_ERR_CUDA            -2   /* a CUDA runtime call failed */
+#define LSP_ERR_NO_DEVICE       -3   /* no CUDA device / wrong architecture */
+#define LSP_ERR_DEVICE_STATUS   -4   /* the device raised an error flag (NaN, index out of range) */
+#define LSP_ERR_NOT_CONVERGED   -5   /* PCISPH hit max iterations above eta (only if strict_convergence) */
+#define LSP_ERR_TIMEOUT         -6   /* a bounded device-side wait gave up */
+#define LSP_ERR_CAPACITY        -7   /* a size exceeds a fixed limit */
+#define LSP_ERR_STATE           -8   /* call not valid in the current state */
+
+/* ---- solver kinds (SPHSolver / PCISPHSolver) ---- */
+#define LSP_SOLVER_SPH     0
+#define LSP_SOLVER_PCISPH  1
+
+/* ---- collider kinds (StaticCollisionObjectType, Collision/StaticCollisionObject.h:6-9) ---- */
+#define LSP_OBSTACLE  0
+#define LSP_BOUNDARY  1
+
+/* ---- warm start of the PCISPH pressure ---- */
+#define LSP_WARM_ZERO      0   /* reference: p = 0, F_p = 0 (PCISPHSolver.cpp:58-62) */
+#define LSP_WARM_MLP       1   /* learned per-particle MLP guess, rejected if it raises the error */
+
+/*
+ * Solver parameters. Field meaning and defaults follow SPHSolver::SPHSolver
+ * (SPHSolver.cpp:11-23) and PCISPHSolver::PCISPHSolver (PCISPHSolver.cpp:6-7);
+ * lsp_params_default() fills exactly those values.
+ */
+typedef struct lsp_params {
+    float gravity[3];                  /* m_gravity, default (0,-9.81,0) */
+    float particle_radius;             /* m_particleRadius, default 0.017 */
+    float kernel_radius_factor;        /* m_kernelRadiusFactor, default 2.688; h = factor * radius */
+    float rest_density;                /* m_restDensity, default 998.29 */
+    float viscosity;                   /* m_viscosityCoefficient, default 3.5 */
+    float stiffness;                   /* m_pressureStiffnessCoefficient, default 3 */
+    float negative_pressure_factor;    /* m_negativePressureFactor, default 0 */
+    float surface_tension;             /* m_surfaceTensionCoefficient, default 0.0728 */
+    float surface_tension_threshold;   /* m_surfaceTensionThreshold, default 7.065 */
+    float restitution;                 /* m_restitutionCoefficient, default 0.5 */
+    float friction;                    /* m_frictionCoefficient, default 1 */
+    float mass_override;               /* <= 0: mass derived as in SPHSolver::recalcParticleMass */
+    int32_t solver;                    /* LSP_SOLVER_SPH or LSP_SOLVER_PCISPH */
+    int32_t pci_max_iterations;        /* the reference's m_minIterations, which bounds the loop from above; default 4 */
+    int32_t pci_min_iterations;        /* extension: no convergence exit before this many; default 1 (= reference) */
+    float pci_eta;                     /* m_maxDensityErrorRatio, default 0.1 */
+    int32_t warm_start;                /* LSP_WARM_*; default LSP_WARM_ZERO */
+    int32_t strict_convergence;        /* 1: lsp_step returns LSP_ERR_NOT_CONVERGED at max iterations */
+    int32_t keep_initial_velocity;     /* 1: skip the reference's first-step velocity wipe in PCISPH (Delta 5) */
+    int32_t reserved[7];
+} lsp_params;
+
+/* Per-step statistics, filled by lsp_step when non-NULL. */
+typedef struct lsp_step_stats {
+    int32_t iterations;               /* PCISPH predict-correct iterations this step (0 for SPH) */
+    int32_t converged;                /* 1 if max density error ratio < eta at exit */
+    double max_density_error_ratio;   /* max |rho* - rho0| / rho0 of the last iteration (compression only when negative_pressure_factor = 0) */
+    int32_t max_neighbors;            /* largest neighbour count this step */
+    int32_t escaped;                  /* particles outside the grid box (clamped into edge cells) */
+    int32_t warm_start_used;          /* 1 if the warm-start guess was kept */
+    int32_t reserved;
+} lsp_step_stats;
+
+/* Fields for lsp_read_field. Vector fields are float[3*n], scalars float[n]. */
+#define LSP_FIELD_POSITION            0
+#define LSP_FIELD_VELOCITY            1
+#define LSP_FIELD_HALF_VELOCITY       2
+#define LSP_FIELD_DENSITY             3
+#define LSP_FIELD_PRESSURE            4
+#define LSP_FIELD_FIRST_STEP          5   /* 1.0 / 0.0 */
+#define LSP_FIELD_PRED_DENSITY        6
+#define LSP_FIELD_DENSITY_ERROR       7
+#define LSP_FIELD_PRED_POSITION       8
+#define LSP_FIELD_PRED_HALF_VELOCITY  9
+#define LSP_FIELD_PRED_PRESSURE_FORCE 10
+#define LSP_FIELD_OLD_HALF_VELOCITY   11
+#define LSP_FIELD_NEIGHBOR_COUNT      12  /* float[n] holding integer counts */
+#define LSP_FIELD_SPEED_SQUARED       13  /* |v|^2, the colour source of SPHParticleDrawable.cpp:10-27 */
+
+typedef struct lsp_solver lsp_solver;
+
+/* ---- lifecycle ---- */
+void lsp_params_default(lsp_params* p);
+const char* lsp_last_error(void);
+int lsp_device_info(int* sm_count, int* cc_major, int* cc_minor);
+
+/* SPHSolver::SPHSolver / PCISPHSolver::PCISPHSolver (SPHSolver.cpp:9-86). device < 0 = current. */
+int lsp_create(const lsp_params* params, int device, lsp_solver** out);
+int lsp_destroy(lsp_solver* s);
+
+/* Setters/getters of SPHSolver.h:79-109 and PCISPHSolver.h:16-20, all at once. */
+int lsp_set_params(lsp_solver* s, const lsp_params* params);
+int lsp_get_params(const lsp_solver* s, lsp_params* out);
+int lsp_particle_mass(const lsp_solver* s, float* mass);          /* getParticleMass */
+int lsp_kernel_radius(const lsp_solver* s, float* h);             /* getKernelRadius */
+int lsp_particle_count(const lsp_solver* s, int64_t* n);          /* getParticleCount */
+int lsp_pcisph_delta(const lsp_solver* s, float dt, float* delta);/* PCISPHSolver::calcDelta (PCISPHSolver.cpp:286-328) */
+/* The 5 x 1001 lookup tables (poly6 W, poly6 dW, poly6 d2W, spiky dW, viscosity d2W),
+ * SPHKernel::recalcCachedWeights (SPHKernel.cpp:113-132). out: float[5*1001]. */
+int lsp_kernel_tables(const lsp_solver* s, float* out, int capacity);
+
+/* ---- scene ---- */
+/* SPHSolver::addParticle (SPHSolver.cpp:129-135), n at a time. vel may be NULL (zero).
+ * New particles start with half-velocity 0 and the first-step flag set (SPHParticle.cpp:4-14). */
+int lsp_add_particles(lsp_solver* s, const float* xyz, const float* vel, int64_t n);
+int lsp_remove_particles(lsp_solver* s);                           /* SPHSolver::removeParticles */
+/* SPHSolver::addStaticCollisionObject with StaticCollisionBox / StaticCollisionSphere.
+ * Colliders act in insertion order, as the CPU solver does (SPHSolver.cpp:376-379). */
+int lsp_add_box(lsp_solver* s, const float center[3], const float half_extent[3], int kind);
+int lsp_add_sphere(lsp_solver* s, const float center[3], float radius, int kind);
+int lsp_remove_colliders(lsp_solver* s);                           /* removeStaticCollisionObjects */
+/* Moves/resizes collider `index` (insertion order); setHasCollisionObjectDataChanged. */
+int lsp_update_box(lsp_solver* s, int index, const float center[3], const float half_extent[3]);
+int lsp_update_sphere(lsp_solver* s, int index, const float center[3], float radius);
+/* Optional grid box. Without it the grid covers the union of boundary boxes, or the
+ * particle bounds at the first step plus a margin. Particles outside are clamped. */
+int lsp_set_domain(lsp_solver* s, const float lo[3], const float hi[3]);
+
+/* ---- stepping ---- */
+/* PhysicSolver::update(dt) (PhysicSolver.cpp:12-21): one full step. */
+int lsp_step(lsp_solver* s, float dt, lsp_step_stats* stats);
+/* n steps back to back without host synchronisation in between (stats of the last). */
+int lsp_step_many(lsp_solver* s, float dt, int steps, lsp_step_stats* stats);
+int lsp_synchronize(lsp_solver* s);
+
+/* ---- read-back / state (caller order) ---- */
+/* Replaces SPHSolver::onEndUpdate's sorted read-back (SPHSolver.cpp:400-427). */
+int lsp_read_particles(lsp_solver* s, float* xyz, float* vel, int64_t n);
+int lsp_read_field(lsp_solver* s, int field, float* out, int64_t n);
+/* Full persistent state: x, v, v_half, v_half_old (float[3n] each) and first-step flags. */
+int lsp_read_state(lsp_solver* s, float* x, float* v, float* half, float* old_half, int32_t* first, int64_t n);
+int lsp_write_state(lsp_solver* s, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first, int64_t n);
+
+/* Start-of-step neighbour lists of the last step, caller order, in the reference's
+ * order (SPHSpatialGrid::findNeighborParticles, SPHSpatialGrid.cpp:39-76).
+ * offsets: int64[n+1]; index: int32[offsets[n]] (pass index=NULL to get offsets only). */
+int lsp_read_neighbors(lsp_solver* s, int64_t* offsets, int32_t* index, int64_t n, int64_t capacity);
+
+/* Grid build of the last step, device order, for parity tests:
+ * cell key and caller id per sorted slot, and the dense cell table (cells+1 entries). */
+int lsp_grid_info(lsp_solver* s, int32_t dims[3], int32_t origin[3], int64_t* cells);
+int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LSP_H */

@@ -1,0 +1,671 @@
+// Host engine: device memory, grid box, step sequencing. See engine.h.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace lsp {
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw Error(LSP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+    } while (0)
+
+// ------------------------------------------------------------------ host kernels
+// SPHKernel::setRadius / recalcCachedWeights (SPHKernel.cpp:93-137) with the poly6,
+// spiky and viscosity formulas (DefaultKernel.cpp:12-42, PressureKernel.cpp:12-42,
+// ViscosityKernel.cpp:12-40); SPHSolver::recalcKernelRadius / recalcParticleMass
+// (SPHSolver.cpp:480-523). Coefficients are formed in double, as M_PI makes them in the
+// reference, and rounded to float.
+void HostKernels::build(const lsp_params& p)
+{
+    const int sub = kTableSize - 1;
+    h = p.kernel_radius_factor * p.particle_radius;
+    float r2 = h * h, r3 = r2 * h, r4 = r3 * h, r5 = r4 * h, r6 = r5 * h, r9 = r6 * r3;
+    (void)r4;
+    step = h / sub;
+    const double pi = 3.14159265358979323846;
+    float poly_k = (float)(315.0 / (64.0 * pi * (double)r9));
+    float poly_d1 = (float)(-945.0 / (32.0 * pi * (double)r9));
+    float poly_d2 = (float)(-945.0 / (32.0 * pi * (double)r9));
+    float spiky_d1 = (float)(-45.0 / (pi * (double)r6));
+    float visc_d2 = (float)(45.0 / (pi * (double)r6));
+    tables.assign(5 * kTableSize, 0.f);
+    for (int i = 0; i <= sub; i++) {
+        float d = i * step;
+        float t = r2 - d * d;
+        tables[0 * kTableSize + i] = poly_k * t * t * t;
+        tables[1 * kTableSize + i] = poly_d1 * t * t;
+        tables[2 * kTableSize + i] = poly_d2 * (r2 - d * d) * (3.f * r2 - 7.f * d * d);
+        float s = h - d;
+        tables[3 * kTableSize + i] = spiky_d1 * s * s;
+        tables[4 * kTableSize + i] = visc_d2 * (h - d);
+    }
+    float stepSize = 1.6f * p.particle_radius;
+    float sum = 0.f;
+    for (int i = -3; i <= 3; i++)
+        for (int j = -3; j <= 3; j++)
+            for (int k = -3; k <= 3; k++) {
+                float x = i * stepSize, y = j * stepSize, z = k * stepSize;
+                sum += look(0, std::sqrt(x * x + y * y + z * z));
+            }
+    mass = p.rest_density / sum;
+    if (p.mass_override > 0.f) mass = p.mass_override;
+}
+
+float HostKernels::look(int t, float d) const
+{
+    if (d >= h) return 0.f;
+    int key = (int)(d / step);
+    return tables[t * kTableSize + key];
+}
+
+// PCISPHSolver::calcDelta (PCISPHSolver.cpp:286-328).
+float HostKernels::delta(const lsp_params& p, float dt) const
+{
+    float stepSize = 1.6f * p.particle_radius;
+    float d1x = 0.f, d1y = 0.f, d1z = 0.f, d2 = 0.f;
+    for (int i = -3; i <= 3; i++)
+        for (int j = -3; j <= 3; j++)
+            for (int k = -3; k <= 3; k++) {
+                float x = i * stepSize, y = j * stepSize, z = k * stepSize;
+                float dist = std::sqrt(x * x + y * y + z * z);
+                if (dist > 0.f) {
+                    float dx = x / dist, dy = y / dist, dz = z / dist;
+                    float w = look(3, dist);
+                    float gx = dx * w, gy = dy * w, gz = dz * w;
+                    d1x += gx; d1y += gy; d1z += gz;
+                    d2 += gx * gx + gy * gy + gz * gz;
+                }
+            }
+    float denom = -(d1x * d1x + d1y * d1y + d1z * d1z) - d2;
+    float beta = dt * mass / p.rest_density;
+    beta = 2.f * beta * beta;
+    float delta = 0.f;
+    if (std::fabs(denom) > 0.f) delta = -1.f / (beta * denom);
+    return delta;
+}
+
+// ------------------------------------------------------------------ device arrays
+template <typename T>
+void DevArray<T>::alloc(size_t count)
+{
+    release();
+    if (count == 0) return;
+    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        p = nullptr;
+        throw Error(e == cudaErrorMemoryAllocation ? LSP_ERR_CAPACITY : LSP_ERR_CUDA,
+                    std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
+                        cudaGetErrorString(e));
+    }
+    n = count;
+}
+
+template <typename T>
+void DevArray<T>::release()
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+}
+
+// ------------------------------------------------------------------ engine
+static void validate(const lsp_params& p)
+{
+    auto bad = [](const char* m) { throw Error(LSP_ERR_INVALID, m); };
+    if (!(p.particle_radius > 0.f) || !std::isfinite(p.particle_radius)) bad("particle_radius must be > 0");
+    if (!(p.kernel_radius_factor > 0.f) || !std::isfinite(p.kernel_radius_factor)) bad("kernel_radius_factor must be > 0");
+    if (!(p.rest_density > 0.f) || !std::isfinite(p.rest_density)) bad("rest_density must be > 0");
+    if (p.solver != LSP_SOLVER_SPH && p.solver != LSP_SOLVER_PCISPH) bad("solver must be LSP_SOLVER_SPH or LSP_SOLVER_PCISPH");
+    if (p.pci_max_iterations < 0 || p.pci_max_iterations > kMaxIterationsCap) bad("pci_max_iterations out of range [0, 1024]");
+    if (p.pci_min_iterations < 0) bad("pci_min_iterations must be >= 0");
+    if (p.warm_start != LSP_WARM_ZERO && p.warm_start != LSP_WARM_MLP) bad("unknown warm_start");
+}
+
+Engine::Engine(const lsp_params& p, int device)
+{
+    validate(p);
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw Error(LSP_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0) CK(cudaGetDevice(&device));
+    if (device >= count) throw Error(LSP_ERR_NO_DEVICE, "device index out of range");
+    dev_ = device;
+    activate();
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, dev_));
+    if (prop.major != 10) throw Error(LSP_ERR_NO_DEVICE, "liblsp is built for sm_100a (B200); device is sm_" +
+                                                             std::to_string(prop.major) + std::to_string(prop.minor));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaMallocHost((void**)&hstatus_, sizeof(DevStatus)));
+    std::memset(hstatus_, 0, sizeof(DevStatus));
+    status_.alloc(1);
+    bounds_.alloc(6);
+    prm_ = p;
+    derive();
+}
+
+Engine::~Engine()
+{
+    cudaSetDevice(dev_);
+    if (stream_) cudaStreamSynchronize(stream_);
+    if (hstatus_) cudaFreeHost(hstatus_);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Engine::activate() const { CK(cudaSetDevice(dev_)); }
+
+void Engine::derive()
+{
+    hk_.build(prm_);
+    tables_dirty_ = true;
+    grid_valid_ = false;   // cell size follows h
+}
+
+void Engine::set_params(const lsp_params& p)
+{
+    validate(p);
+    bool geometry = p.particle_radius != prm_.particle_radius || p.kernel_radius_factor != prm_.kernel_radius_factor;
+    prm_ = p;
+    derive();
+    if (geometry) nbr_cap_ = 0;  // re-estimate the list capacity for the new h
+}
+
+static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+void Engine::ensure_capacity(int64_t n)
+{
+    if (n <= cap_) return;
+    activate();
+    int64_t cap = round_up(std::max<int64_t>(n, cap_ + cap_ / 2), 256);
+    DevArray<float4> np[4];
+    DevArray<int32_t> nsoi;
+    for (int k = 0; k < 4; k++) np[k].alloc(cap);
+    nsoi.alloc(cap);
+    DevArray<float4>* cur[4] = {&pos_[cur_], &vel_[cur_], &half_[cur_], &old_[cur_]};
+    if (n_ > 0) {
+        for (int k = 0; k < 4; k++)
+            CK(cudaMemcpyAsync(np[k].p, cur[k]->p, n_ * sizeof(float4), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(nsoi.p, slot_of_id_.p, n_ * sizeof(int32_t), cudaMemcpyDeviceToDevice, stream_));
+    }
+    CK(cudaStreamSynchronize(stream_));
+    for (int k = 0; k < 4; k++) std::swap(cur[k]->p, np[k].p), std::swap(cur[k]->n, np[k].n);
+    std::swap(slot_of_id_.p, nsoi.p), std::swap(slot_of_id_.n, nsoi.n);
+    for (int k = 0; k < 4; k++) np[k].release();
+    pos_[1 - cur_].alloc(cap); vel_[1 - cur_].alloc(cap); half_[1 - cur_].alloc(cap); old_[1 - cur_].alloc(cap);
+    force_.alloc(cap); ppos_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
+    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap); sfac_.alloc(cap);
+    key_.alloc(cap); slot_.alloc(cap); sorted_key_.alloc(cap); tmp_.alloc(cap); nbr_count_.alloc(cap);
+    stage_.alloc(cap * 12);
+    CK(cudaMemsetAsync(force_.p, 0, cap * sizeof(float4), stream_));
+    CK(cudaMemsetAsync(ppos_.p, 0, cap * sizeof(float4), stream_));
+    CK(cudaMemsetAsync(phalf_.p, 0, cap * sizeof(float4), stream_));
+    CK(cudaMemsetAsync(pforce_.p, 0, cap * sizeof(float4), stream_));
+    for (DevArray<float>* a : {&rho_, &pres_, &prho_, &err_, &sfac_})
+        CK(cudaMemsetAsync(a->p, 0, cap * sizeof(float), stream_));
+    CK(cudaMemsetAsync(nbr_count_.p, 0, cap * sizeof(int32_t), stream_));
+    cap_ = cap;
+    if (nbr_cap_ > 0) ensure_neighbors(nbr_cap_);
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::ensure_neighbors(int cap)
+{
+    cap = (int)round_up(std::max(cap, 16), 8);
+    if (cap > 4096) throw Error(LSP_ERR_CAPACITY, "neighbour count above 4096 per particle");
+    nbr_stride_ = std::max<int64_t>(cap_, 256);
+    nbr_.alloc((size_t)cap * (size_t)nbr_stride_);
+    nbr_cap_ = cap;
+}
+
+void Engine::add_particles(const float* xyz, const float* vel, int64_t m)
+{
+    if (m < 0 || (m > 0 && !xyz)) throw Error(LSP_ERR_INVALID, "add_particles: bad pointer or count");
+    if (m == 0) return;
+    if (n_ + m > (int64_t)INT32_MAX / 2) throw Error(LSP_ERR_CAPACITY, "particle count above 2^30");
+    ensure_capacity(n_ + m);
+    std::vector<float4> p(m), v(m), z(m, make_float4(0.f, 0.f, 0.f, 0.f));
+    std::vector<int32_t> soi(m);
+    for (int64_t i = 0; i < m; i++) {
+        int32_t id = (int32_t)(n_ + i);
+        float w;
+        std::memcpy(&w, &id, 4);
+        p[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], w);
+        v[i] = vel ? make_float4(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2], 1.f) : make_float4(0.f, 0.f, 0.f, 1.f);
+        soi[i] = id;
+    }
+    activate();
+    CK(cudaMemcpyAsync(pos_[cur_].p + n_, p.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(vel_[cur_].p + n_, v.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(half_[cur_].p + n_, z.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(old_[cur_].p + n_, z.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(slot_of_id_.p + n_, soi.data(), m * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    n_ += m;
+    if (domain_from_particles_) grid_valid_ = false;
+}
+
+void Engine::remove_particles()
+{
+    n_ = 0;
+    if (domain_from_particles_) grid_valid_ = false;
+}
+
+int Engine::add_collider(const Collider& c)
+{
+    if ((int)cols_.size() >= kMaxColliders) throw Error(LSP_ERR_CAPACITY, "more than 64 colliders");
+    cols_.push_back(c);
+    cols_dirty_ = true;
+    if (!domain_user_ && c.boundary) grid_valid_ = false;
+    return (int)cols_.size() - 1;
+}
+
+void Engine::update_collider(int index, const Collider& c)
+{
+    if (index < 0 || index >= (int)cols_.size()) throw Error(LSP_ERR_INVALID, "collider index out of range");
+    if (cols_[index].sphere != c.sphere) throw Error(LSP_ERR_INVALID, "collider kind mismatch");
+    Collider u = c;
+    u.boundary = cols_[index].boundary;
+    cols_[index] = u;
+    cols_dirty_ = true;
+}
+
+void Engine::remove_colliders()
+{
+    cols_.clear();
+    cols_dirty_ = true;
+    if (!domain_user_) grid_valid_ = false;
+}
+
+void Engine::set_domain(const float lo[3], const float hi[3])
+{
+    for (int a = 0; a < 3; a++)
+        if (!(hi[a] >= lo[a]) || !std::isfinite(lo[a]) || !std::isfinite(hi[a]))
+            throw Error(LSP_ERR_INVALID, "domain: need finite lo <= hi");
+    std::memcpy(dom_lo_, lo, sizeof(dom_lo_));
+    std::memcpy(dom_hi_, hi, sizeof(dom_hi_));
+    domain_user_ = true;
+    grid_valid_ = false;
+}
+
+void Engine::upload_colliders()
+{
+    activate();
+    if (dcols_.n < (size_t)kMaxColliders) dcols_.alloc(kMaxColliders);
+    if (!cols_.empty())
+        CK(cudaMemcpyAsync(dcols_.p, cols_.data(), cols_.size() * sizeof(Collider), cudaMemcpyHostToDevice, stream_));
+    cols_dirty_ = false;
+}
+
+// Grid box: the user domain, else the union of boundary colliders, else the particle
+// bounds plus a margin. Cells are the reference CPU grid's, c = (int)(x / h).
+void Engine::ensure_grid()
+{
+    if (grid_valid_) return;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    bool have = false;
+    domain_from_particles_ = false;
+    if (domain_user_) {
+        std::memcpy(lo, dom_lo_, sizeof(lo));
+        std::memcpy(hi, dom_hi_, sizeof(hi));
+        have = true;
+    } else {
+        for (const Collider& c : cols_) {
+            if (!c.boundary) continue;
+            float cc[3] = {c.cx, c.cy, c.cz};
+            float e[3] = {c.hx, c.hy, c.hz};
+            if (c.sphere) e[0] = e[1] = e[2] = c.radius;
+            for (int a = 0; a < 3; a++) {
+                float l = cc[a] - std::fabs(e[a]), u = cc[a] + std::fabs(e[a]);
+                lo[a] = have ? std::min(lo[a], l) : l;
+                hi[a] = have ? std::max(hi[a], u) : u;
+            }
+            have = true;
+        }
+    }
+    if (!have && n_ > 0) {
+        activate();
+        int32_t init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, INT32_MIN, INT32_MIN, INT32_MIN};
+        CK(cudaMemcpyAsync(bounds_.p, init, sizeof(init), cudaMemcpyHostToDevice, stream_));
+        launch_bounds(pos_[cur_].p, n_, bounds_.p, stream_);
+        int32_t out[6];
+        CK(cudaMemcpyAsync(out, bounds_.p, sizeof(out), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        for (int a = 0; a < 6; a++) {
+            int32_t v = out[a] >= 0 ? out[a] : (out[a] ^ 0x7fffffff);
+            float f;
+            std::memcpy(&f, &v, 4);
+            if (a < 3) lo[a] = f; else hi[a - 3] = f;
+        }
+        for (int a = 0; a < 3; a++) {
+            if (!(lo[a] <= hi[a])) { lo[a] = 0.f; hi[a] = 0.f; }
+            float margin = std::max(0.25f * (hi[a] - lo[a]), 4.f * hk_.h);
+            lo[a] -= margin;
+            hi[a] += margin;
+        }
+        domain_from_particles_ = true;
+    }
+    int64_t cells = 1;
+    for (int a = 0; a < 3; a++) {
+        int c0 = (int)(lo[a] / hk_.h), c1 = (int)(hi[a] / hk_.h);
+        org_[a] = c0;
+        dim_[a] = std::max(1, c1 - c0 + 1);
+        cells *= dim_[a];
+    }
+    if (cells > ((int64_t)1 << 30)) throw Error(LSP_ERR_CAPACITY, "grid box holds more than 2^30 cells of size h");
+    cells_ = cells;
+    if (cells + 1 > cells_alloc_) {
+        activate();
+        int64_t alloc = cells + 1;
+        hist_.alloc(alloc);
+        cell_start_.alloc(alloc);
+        tile_sums_.alloc((alloc + 2047) / 2048 + 1);
+        CK(cudaMemsetAsync(hist_.p, 0, alloc * sizeof(uint32_t), stream_));
+        CK(cudaMemsetAsync(cell_start_.p, 0, alloc * sizeof(uint32_t), stream_));
+        cells_alloc_ = alloc;
+    }
+    grid_valid_ = true;
+}
+
+DevParams Engine::device_params(float dt) const
+{
+    DevParams P{};
+    P.gx = prm_.gravity[0]; P.gy = prm_.gravity[1]; P.gz = prm_.gravity[2];
+    P.h = hk_.h;
+    P.h2 = hk_.h * hk_.h;
+    P.step = hk_.step;
+    P.radius = prm_.particle_radius;
+    P.mass = hk_.mass;
+    P.rho0 = prm_.rest_density;
+    P.stiffness = prm_.stiffness;
+    P.neg = prm_.negative_pressure_factor;
+    P.viscosity = prm_.viscosity;
+    P.sigma = prm_.surface_tension;
+    P.sigma_thr = prm_.surface_tension_threshold;
+    P.restitution = prm_.restitution;
+    P.friction = prm_.friction;
+    P.delta = prm_.solver == LSP_SOLVER_PCISPH ? hk_.delta(prm_, dt) : 0.f;
+    P.eta = prm_.pci_eta;
+    P.dt = dt;
+    P.n = (int)n_;
+    P.keep_initial_velocity = prm_.keep_initial_velocity;
+    P.ncoll = (int)cols_.size();
+    P.ox = org_[0]; P.oy = org_[1]; P.oz = org_[2];
+    P.nx = dim_[0]; P.ny = dim_[1]; P.nz = dim_[2];
+    P.cells = (uint32_t)cells_;
+    P.nbr_cap = nbr_cap_;
+    P.nbr_stride = nbr_stride_;
+    P.min_it = prm_.pci_min_iterations;
+    P.max_it = prm_.pci_max_iterations;
+    return P;
+}
+
+StepBuffers Engine::buffers()
+{
+    StepBuffers b{};
+    b.pos = pos_[cur_].p; b.vel = vel_[cur_].p; b.half = half_[cur_].p; b.old = old_[cur_].p;
+    b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
+    b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p; b.sfac = sfac_.p;
+    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
+    b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p;
+    return b;
+}
+
+void Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st)
+{
+    int it = 0;
+    bool conv = false;
+    float maxErr = 0.f, ratio = 0.f;
+    if (P.max_it <= 0) CK(cudaMemsetAsync(pforce_.p, 0, n_ * sizeof(float4), stream_));
+    for (int k = 0; k < P.max_it; k++) {
+        launch_pci_predict(P, b, k, stream_);
+        launch_pci_density(P, b, k, stream_);
+        launch_pci_force(P, b, stream_);
+        it = k + 1;
+        CK(cudaMemcpyAsync(&hstatus_->max_err_bits, &status_.p->max_err_bits, sizeof(uint32_t),
+                           cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        std::memcpy(&maxErr, &hstatus_->max_err_bits, 4);
+        ratio = maxErr / prm_.rest_density;
+        conv = std::fabs(ratio) < prm_.pci_eta;
+        if (conv && it >= P.min_it) break;
+    }
+    if (st) {
+        st->iterations = it;
+        st->converged = conv ? 1 : 0;
+        st->max_density_error_ratio = (double)maxErr / (double)prm_.rest_density;
+    }
+}
+
+static int initial_neighbor_capacity(const lsp_params& p)
+{
+    // Lattice estimate (4/3) pi (h/s)^3 with s = 1.6 r, doubled for compression.
+    double q = p.kernel_radius_factor / 1.6;
+    double est = 4.18879 * q * q * q;
+    return (int)std::min(4096.0, std::ceil(2.0 * est) + 16.0);
+}
+
+void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
+{
+    (void)final_sync;
+    if (st) std::memset(st, 0, sizeof(*st));
+    if (!(dt > 0.f) || !std::isfinite(dt)) throw Error(LSP_ERR_INVALID, "dt must be finite and > 0");
+    if (n_ == 0) {
+        if (st) st->converged = 1;
+        return;
+    }
+    activate();
+    ensure_grid();
+    if (cols_dirty_) upload_colliders();
+    if (tables_dirty_) {
+        if (!tables_.p) tables_.alloc(5 * kTableSize);
+        CK(cudaMemcpyAsync(tables_.p, hk_.tables.data(), 5 * kTableSize * sizeof(float), cudaMemcpyHostToDevice,
+                           stream_));
+        tables_dirty_ = false;
+    }
+    if (!dcols_.p) upload_colliders();
+    if (nbr_cap_ == 0 || nbr_stride_ < cap_) ensure_neighbors(nbr_cap_ ? nbr_cap_ : initial_neighbor_capacity(prm_));
+    lsp_step_stats local{};
+    for (int attempt = 0;; attempt++) {
+        DevParams P = device_params(dt);
+        CK(cudaMemsetAsync(status_.p, 0, sizeof(DevStatus), stream_));
+        GridBuildArgs g{};
+        g.P = P;
+        g.pos_in = pos_[cur_].p; g.vel_in = vel_[cur_].p; g.half_in = half_[cur_].p; g.old_in = old_[cur_].p;
+        g.pos_out = pos_[1 - cur_].p; g.vel_out = vel_[1 - cur_].p;
+        g.half_out = half_[1 - cur_].p; g.old_out = old_[1 - cur_].p;
+        g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
+        g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
+        g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
+        launch_grid_build(g, stream_);
+        cur_ = 1 - cur_;
+        StepBuffers b = buffers();
+        launch_density(P, b, stream_);
+        launch_nonpressure(P, b, stream_);
+        if (prm_.solver == LSP_SOLVER_SPH) {
+            launch_sph_pressure(P, b, stream_);
+            launch_integrate_collide(P, b, false, stream_);
+            local.iterations = 0;
+            local.converged = 1;
+        } else {
+            pcisph_loop(P, b, &local);
+            launch_integrate_collide(P, b, true, stream_);
+        }
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hstatus_, status_.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        if ((hstatus_->error_flags & kErrNeighborOverflow) && attempt < 3) {
+            cur_ = 1 - cur_;   // the gather left the pre-step state untouched: redo the step
+            ensure_neighbors((int)hstatus_->max_neighbors + (int)hstatus_->max_neighbors / 4 + 8);
+            continue;
+        }
+        break;
+    }
+    stepped_ = true;
+    local.max_neighbors = (int32_t)hstatus_->max_neighbors;
+    local.escaped = (int32_t)hstatus_->escaped;
+    if (st) *st = local;
+    if (hstatus_->escaped && domain_from_particles_) grid_valid_ = false;
+    if (hstatus_->error_flags & kErrNeighborOverflow)
+        throw Error(LSP_ERR_CAPACITY, "neighbour list overflow persisted after resizing");
+    if (hstatus_->error_flags & kErrScan)
+        throw Error(LSP_ERR_CAPACITY, "a grid cell holds more than 4096 particles");
+    if (hstatus_->error_flags & kErrNaN)
+        throw Error(LSP_ERR_DEVICE_STATUS, "non-finite particle position at the start of the step");
+    if (prm_.solver == LSP_SOLVER_PCISPH && prm_.strict_convergence && !local.converged)
+        throw Error(LSP_ERR_NOT_CONVERGED, "PCISPH reached max iterations above eta");
+}
+
+void Engine::step(float dt, lsp_step_stats* st) { run_step(dt, st, true); }
+
+void Engine::step_many(float dt, int steps, lsp_step_stats* st)
+{
+    if (steps < 0) throw Error(LSP_ERR_INVALID, "steps must be >= 0");
+    for (int s = 0; s < steps; s++) run_step(dt, st, s == steps - 1);
+}
+
+void Engine::synchronize()
+{
+    activate();
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::stage(size_t floats)
+{
+    if (stage_.n < floats) stage_.alloc(floats);
+}
+
+void Engine::read_field(int field, float* out, int64_t n)
+{
+    if (!out || n != n_) throw Error(LSP_ERR_INVALID, "read_field: n must equal the particle count");
+    if (n == 0) return;
+    activate();
+    const void* src = nullptr;
+    int comps = 1, mode = 0;
+    switch (field) {
+    case LSP_FIELD_POSITION: src = pos_[cur_].p; comps = 3; break;
+    case LSP_FIELD_VELOCITY: src = vel_[cur_].p; comps = 3; break;
+    case LSP_FIELD_HALF_VELOCITY: src = half_[cur_].p; comps = 3; break;
+    case LSP_FIELD_OLD_HALF_VELOCITY: src = old_[cur_].p; comps = 3; break;
+    case LSP_FIELD_PRED_POSITION: src = ppos_.p; comps = 3; break;
+    case LSP_FIELD_PRED_HALF_VELOCITY: src = phalf_.p; comps = 3; break;
+    case LSP_FIELD_PRED_PRESSURE_FORCE: src = pforce_.p; comps = 3; break;
+    case LSP_FIELD_DENSITY: src = rho_.p; break;
+    case LSP_FIELD_PRESSURE: src = pres_.p; break;
+    case LSP_FIELD_PRED_DENSITY: src = prho_.p; break;
+    case LSP_FIELD_DENSITY_ERROR: src = err_.p; break;
+    case LSP_FIELD_FIRST_STEP: src = vel_[cur_].p; mode = 1; break;
+    case LSP_FIELD_SPEED_SQUARED: src = vel_[cur_].p; mode = 2; break;
+    case LSP_FIELD_NEIGHBOR_COUNT: break;
+    default: throw Error(LSP_ERR_INVALID, "unknown field");
+    }
+    stage((size_t)n * comps);
+    if (field == LSP_FIELD_NEIGHBOR_COUNT)
+        launch_gather_count(nbr_count_.p, slot_of_id_.p, stage_.p, n, stream_);
+    else
+        launch_gather_field(src, comps, mode, slot_of_id_.p, stage_.p, n, stream_);
+    CK(cudaMemcpyAsync(out, stage_.p, (size_t)n * comps * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::read_state(float* x, float* v, float* half, float* old, int32_t* first, int64_t n)
+{
+    if (n != n_ || !x || !v || !half || !old || !first) throw Error(LSP_ERR_INVALID, "read_state: bad arguments");
+    if (n == 0) return;
+    activate();
+    stage((size_t)n * 13);
+    float* s = stage_.p;
+    launch_gather_state(pos_[cur_].p, vel_[cur_].p, half_[cur_].p, old_[cur_].p, slot_of_id_.p, s, s + 3 * n,
+                        s + 6 * n, s + 9 * n, (int32_t*)(s + 12 * n), n, stream_);
+    size_t b3 = (size_t)n * 3 * sizeof(float);
+    CK(cudaMemcpyAsync(x, s, b3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(v, s + 3 * n, b3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(half, s + 6 * n, b3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(old, s + 9 * n, b3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(first, s + 12 * n, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::write_state(const float* x, const float* v, const float* half, const float* old, const int32_t* first,
+                         int64_t n)
+{
+    if (n != n_ || !x || !v || !half || !old || !first) throw Error(LSP_ERR_INVALID, "write_state: bad arguments");
+    if (n == 0) return;
+    activate();
+    stage((size_t)n * 13);
+    float* s = stage_.p;
+    size_t b3 = (size_t)n * 3 * sizeof(float);
+    CK(cudaMemcpyAsync(s, x, b3, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(s + 3 * n, v, b3, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(s + 6 * n, half, b3, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(s + 9 * n, old, b3, cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(s + 12 * n, first, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+    launch_scatter_state(s, s + 3 * n, s + 6 * n, s + 9 * n, (const int32_t*)(s + 12 * n), slot_of_id_.p,
+                         pos_[cur_].p, vel_[cur_].p, half_[cur_].p, old_[cur_].p, n, stream_);
+    CK(cudaStreamSynchronize(stream_));
+    if (domain_from_particles_) grid_valid_ = false;
+}
+
+void Engine::read_neighbors(int64_t* offsets, int32_t* index, int64_t n, int64_t capacity)
+{
+    if (n != n_ || !offsets) throw Error(LSP_ERR_INVALID, "read_neighbors: bad arguments");
+    if (!stepped_) throw Error(LSP_ERR_STATE, "read_neighbors: no step has run");
+    std::vector<float> counts(n);
+    read_field(LSP_FIELD_NEIGHBOR_COUNT, counts.data(), n);
+    offsets[0] = 0;
+    for (int64_t i = 0; i < n; i++) offsets[i + 1] = offsets[i] + (int64_t)counts[i];
+    if (!index) return;
+    if (capacity < offsets[n]) throw Error(LSP_ERR_INVALID, "read_neighbors: index capacity too small");
+    activate();
+    DevArray<int64_t> doff;
+    DevArray<int32_t> dout;
+    doff.alloc(n + 1);
+    dout.alloc(std::max<int64_t>(offsets[n], 1));
+    CK(cudaMemcpyAsync(doff.p, offsets, (n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream_));
+    launch_neighbor_export(nbr_.p, nbr_count_.p, nbr_stride_, pos_[cur_].p, slot_of_id_.p, doff.p, dout.p, n, stream_);
+    CK(cudaMemcpyAsync(index, dout.p, offsets[n] * sizeof(int32_t), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::grid_info(int32_t dims[3], int32_t origin[3], int64_t* cells) const
+{
+    for (int a = 0; a < 3; a++) {
+        if (dims) dims[a] = dim_[a];
+        if (origin) origin[a] = org_[a];
+    }
+    if (cells) *cells = cells_;
+}
+
+void Engine::read_grid(uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one)
+{
+    if (n != n_) throw Error(LSP_ERR_INVALID, "read_grid: n must equal the particle count");
+    if (!stepped_) throw Error(LSP_ERR_STATE, "read_grid: no step has run");
+    activate();
+    if (keys) CK(cudaMemcpyAsync(keys, sorted_key_.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_));
+    if (ids) {
+        std::vector<float4> p(n);
+        CK(cudaMemcpyAsync(p.data(), pos_[cur_].p, n * sizeof(float4), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        for (int64_t i = 0; i < n; i++) std::memcpy(&ids[i], &p[i].w, 4);
+    }
+    if (cell_start) {
+        if (cells_plus_one != cells_ + 1) throw Error(LSP_ERR_INVALID, "read_grid: cell table size mismatch");
+        CK(cudaMemcpyAsync(cell_start, cell_start_.p, cells_plus_one * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                           stream_));
+    }
+    CK(cudaStreamSynchronize(stream_));
+}
+
+template struct DevArray<float4>;
+template struct DevArray<float>;
+template struct DevArray<uint32_t>;
+template struct DevArray<int32_t>;
+template struct DevArray<int64_t>;
+template struct DevArray<int2>;
+template struct DevArray<Collider>;
+template struct DevArray<DevStatus>;
+
+}  // namespace lsp

@@ -1,0 +1,125 @@
+// Host engine behind the C ABI: owns one scene's device memory and CUDA stream and
+// sequences the per-step kernels (PhysicSolver::update, PhysicSolver.cpp:12-21).
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/lsp.h"
+#include "lsp_kernels.h"
+
+namespace lsp {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+// Reference-identical host arithmetic (compiled with -ffp-contract=off).
+struct HostKernels {
+    float h = 0, step = 0, mass = 0;
+    std::vector<float> tables;   // 5 x 1001
+    void build(const lsp_params& p);
+    float delta(const lsp_params& p, float dt) const;
+    float look(int t, float d) const;
+};
+
+template <typename T>
+struct DevArray {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count);
+    void release();
+    ~DevArray() { release(); }
+};
+
+class Engine {
+public:
+    Engine(const lsp_params& p, int device);
+    ~Engine();
+
+    void set_params(const lsp_params& p);
+    const lsp_params& params() const { return prm_; }
+    float mass() const { return hk_.mass; }
+    float kernel_radius() const { return hk_.h; }
+    float delta(float dt) const { return hk_.delta(prm_, dt); }
+    const std::vector<float>& tables() const { return hk_.tables; }
+    int64_t count() const { return n_; }
+
+    void add_particles(const float* xyz, const float* vel, int64_t m);
+    void remove_particles();
+    int add_collider(const Collider& c);
+    void update_collider(int index, const Collider& c);
+    void remove_colliders();
+    const std::vector<Collider>& colliders() const { return cols_; }
+    void set_domain(const float lo[3], const float hi[3]);
+
+    void step(float dt, lsp_step_stats* st);
+    void step_many(float dt, int steps, lsp_step_stats* st);
+    void synchronize();
+
+    void read_field(int field, float* out, int64_t n);
+    void read_state(float* x, float* v, float* half, float* old, int32_t* first, int64_t n);
+    void write_state(const float* x, const float* v, const float* half, const float* old, const int32_t* first,
+                     int64_t n);
+    void read_neighbors(int64_t* offsets, int32_t* index, int64_t n, int64_t capacity);
+    void grid_info(int32_t dims[3], int32_t origin[3], int64_t* cells) const;
+    void read_grid(uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one);
+
+    cudaStream_t stream() const { return stream_; }
+    int device() const { return dev_; }
+    // Device order view for in-library callers (kernel timing, the MLP).
+    StepBuffers buffers();
+    DevParams device_params(float dt) const;
+
+private:
+    void activate() const;
+    void derive();
+    void ensure_capacity(int64_t n);
+    void ensure_grid();
+    void ensure_neighbors(int cap);
+    void upload_colliders();
+    void run_step(float dt, lsp_step_stats* st, bool final_sync);
+    void pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st);
+    void stage(size_t floats);
+
+    lsp_params prm_{};
+    HostKernels hk_;
+    int dev_ = 0;
+    cudaStream_t stream_ = nullptr;
+
+    int64_t n_ = 0, cap_ = 0;
+    int cur_ = 0;
+    DevArray<float4> pos_[2], vel_[2], half_[2], old_[2];
+    DevArray<float4> force_, ppos_, phalf_, pforce_;
+    DevArray<float> rho_, pres_, prho_, err_, sfac_;
+    DevArray<uint32_t> key_, slot_, sorted_key_;
+    DevArray<int2> tmp_;
+    DevArray<int32_t> slot_of_id_, nbr_, nbr_count_;
+    int nbr_cap_ = 0;
+    int64_t nbr_stride_ = 0;
+
+    DevArray<uint32_t> hist_, cell_start_, tile_sums_;
+    int64_t cells_alloc_ = 0;
+    bool grid_valid_ = false, domain_user_ = false, domain_from_particles_ = false;
+    float dom_lo_[3] = {0, 0, 0}, dom_hi_[3] = {0, 0, 0};
+    int32_t org_[3] = {0, 0, 0}, dim_[3] = {1, 1, 1};
+    int64_t cells_ = 1;
+
+    DevArray<float> tables_;
+    DevArray<Collider> dcols_;
+    std::vector<Collider> cols_;
+    bool cols_dirty_ = true, tables_dirty_ = true;
+
+    DevArray<DevStatus> status_;
+    DevStatus* hstatus_ = nullptr;   // pinned
+    DevArray<float> stage_;
+    DevArray<int32_t> bounds_;
+    bool stepped_ = false;
+};
+
+}  // namespace lsp

@@ -1,0 +1,288 @@
+// Uniform-grid build: cell keys, counting sort by (cell, caller id), particle reorder,
+// dense cell table, and the start-of-step neighbour lists.
+//
+// Replaces the reference's per-step grid build, both its CPU hash grid
+// (SPHSpatialGrid.cpp:19-90, via SPHSolver.cpp:431-440) and its OpenCL grid
+// (calcGridIndices / countDigitsInBuckets / permuteParticles / buildCellList,
+// SPHKernels.cl:66-186 with the host scan at SPHSolver.cpp:1052-1119).
+//
+// Cells are the CPU grid's cells, c = (int)(x / h) per axis, inside a fixed grid box;
+// the key orders them x slowest, z fastest, which is the order in which the CPU's
+// neighbour search visits cells. Sorting by (key, caller id) therefore lays out every
+// 3-cell z-run of the 3x3 row neighbourhood as one contiguous range, in exactly the
+// CPU's visiting order, so neighbour lists come out in the reference's order.
+//
+// The sort is a counting sort (a radix sort whose single digit is the whole cell key):
+//   k_keys_hist   key per particle; warp-aggregated histogram (__match_any_sync) with slots
+//   k_scan_*      exclusive scan of the histogram = dense cell table (lower bounds)
+//   k_scatter     particle -> (cell start + slot)
+//   k_rank_gather deterministic rank by caller id inside each cell, then one gather of
+//                 the 64-byte persistent state into the new order
+//   k_neighbors   the start-of-step neighbour lists, column-major, reference order
+#include "lsp_device.cuh"
+#include "lsp_kernels.h"
+
+namespace lsp {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+constexpr int kMaxCellOccupancy = 4096;
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+__global__ void k_keys_hist(DevParams P, const float4* __restrict__ pos, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ slot, uint32_t* __restrict__ hist, DevStatus* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    const int lane = threadIdx.x & 31;
+    uint32_t k = 0xffffffffu;
+    bool escaped = false, bad = false;
+    if (valid) {
+        float4 p = pos[i];
+        bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+        int c[3] = {cell_coord(p.x, P.h), cell_coord(p.y, P.h), cell_coord(p.z, P.h)};
+        const int o[3] = {P.ox, P.oy, P.oz};
+        const int d[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            int v = c[a];
+            if (v < o[a]) { v = o[a]; escaped = true; }
+            if (v > o[a] + d[a] - 1) { v = o[a] + d[a] - 1; escaped = true; }
+            c[a] = v - o[a];
+        }
+        k = (uint32_t)(((uint32_t)c[0] * (uint32_t)P.ny + (uint32_t)c[1]) * (uint32_t)P.nz + (uint32_t)c[2]);
+    }
+    // Warp-aggregated histogram: one atomic per distinct key in the warp; lanes with the
+    // same key take consecutive slots in lane order.
+    uint32_t peers = __match_any_sync(0xffffffffu, k);
+    uint32_t leader = __ffs(peers) - 1;
+    uint32_t rank = __popc(peers & lanemask_lt());
+    uint32_t base = 0;
+    if (valid && lane == (int)leader) base = atomicAdd(&hist[k], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (valid) {
+        key[i] = k;
+        slot[i] = base + rank;
+    }
+    uint32_t esc = __ballot_sync(0xffffffffu, valid && escaped);
+    uint32_t nan = __ballot_sync(0xffffffffu, valid && bad);
+    if (lane == 0) {
+        if (esc) atomicAdd(&st->escaped, (uint32_t)__popc(esc));
+        if (nan) atomicOr(&st->error_flags, kErrNaN);
+    }
+}
+
+// Block-wide exclusive scan of kScanItems consecutive items per thread, warp shuffles
+// inside each warp, then the warp totals.
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums, uint32_t* total)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    uint32_t warp_prefix = warp ? warp_sums[warp - 1] : 0u;
+    if (total) *total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return warp_prefix + x - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, int64_t n,
+                                                             uint32_t* __restrict__ tile_sums)
+{
+    __shared__ uint32_t ws[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++)
+        if (base + j < n) s += in[base + j];
+    uint32_t total;
+    block_exclusive_scan(s, ws, &total);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One block scans the tile sums in place (exclusive), chunk by chunk with a carry.
+__global__ void __launch_bounds__(1024) k_scan_top(uint32_t* tile_sums, int tiles)
+{
+    __shared__ uint32_t ws[32];
+    uint32_t carry = 0;
+    for (int b = 0; b < tiles; b += blockDim.x) {
+        int i = b + threadIdx.x;
+        uint32_t v = i < tiles ? tile_sums[i] : 0u;
+        uint32_t total;
+        uint32_t ex = block_exclusive_scan(v, ws, &total);
+        if (i < tiles) tile_sums[i] = carry + ex;
+        carry += total;
+        __syncthreads();
+    }
+}
+
+// Exclusive scan of the histogram into the dense cell table; clears the histogram for
+// the next step.
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restrict__ hist, int64_t n,
+                                                             const uint32_t* __restrict__ tile_sums,
+                                                             uint32_t* __restrict__ out)
+{
+    __shared__ uint32_t ws[32];
+    const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        v[j] = base + j < n ? hist[base + j] : 0u;
+        s += v[j];
+    }
+    uint32_t ex = block_exclusive_scan(s, ws, nullptr) + tile_sums[blockIdx.x];
+#pragma unroll
+    for (int j = 0; j < kScanItems; j++) {
+        if (base + j < n) {
+            out[base + j] = ex;
+            hist[base + j] = 0u;
+        }
+        ex += v[j];
+    }
+}
+
+__global__ void k_scatter(DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ key,
+                          const uint32_t* __restrict__ slot, const uint32_t* __restrict__ cell_start,
+                          int2* __restrict__ tmp)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    uint32_t k = key[i];
+    tmp[cell_start[k] + slot[i]] = make_int2(i, id_of(pos[i]));
+}
+
+// Final slot = cell start + number of particles of the same cell with a smaller caller id.
+// Then moves the particle's persistent state (x|id, v|first, v_half|p1, v_half_old|p2).
+__global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const uint32_t* __restrict__ key,
+                              const uint32_t* __restrict__ cell_start,
+                              const float4* __restrict__ ipos, const float4* __restrict__ ivel,
+                              const float4* __restrict__ ihalf, const float4* __restrict__ iold,
+                              float4* __restrict__ opos, float4* __restrict__ ovel,
+                              float4* __restrict__ ohalf, float4* __restrict__ oold,
+                              int32_t* __restrict__ slot_of_id, uint32_t* __restrict__ sorted_key, DevStatus* st)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P.n) return;
+    int2 e = tmp[p];
+    uint32_t k = key[e.x];
+    uint32_t beg = cell_start[k], end = cell_start[k + 1];
+    uint32_t rank = 0;
+    if (end - beg <= (uint32_t)kMaxCellOccupancy) {
+        for (uint32_t q = beg; q < end; q++) rank += tmp[q].y < e.y ? 1u : 0u;
+    } else {
+        rank = (uint32_t)p - beg;   // order inside an overfull cell is not the reference's
+        atomicOr(&st->error_flags, kErrScan);
+    }
+    uint32_t dest = beg + rank;
+    opos[dest] = ipos[e.x];
+    ovel[dest] = ivel[e.x];
+    ohalf[dest] = ihalf[e.x];
+    oold[dest] = iold[e.x];
+    slot_of_id[e.y] = (int32_t)dest;
+    sorted_key[dest] = k;
+}
+
+// Start-of-step neighbour list of each particle: every j with |x_i - x_j|^2 <= h^2,
+// including i, in the reference's order (SPHSpatialGrid::findNeighborParticles,
+// SPHSpatialGrid.cpp:39-76): cell ranges from (x -+ h) / h per axis, x then y rows,
+// each row a contiguous z-run of the sorted array.
+__global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ cell_start,
+                            int32_t* __restrict__ nbr, int32_t* __restrict__ count, DevStatus* st)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    int c = 0;
+    if (valid) {
+        const float4 pi = pos[i];
+        const V3 xi = v3(pi);
+        const float h = P.h;
+        int lo[3] = {(int)((xi.x - h) / h), (int)((xi.y - h) / h), (int)((xi.z - h) / h)};
+        int hi[3] = {(int)((xi.x + h) / h), (int)((xi.y + h) / h), (int)((xi.z + h) / h)};
+        const int o[3] = {P.ox, P.oy, P.oz};
+        const int d[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            // Both ends clamped into the box: a particle outside it searches the edge
+            // cell that holds every clamped particle.
+            lo[a] = min(max(lo[a], o[a]), o[a] + d[a] - 1) - o[a];
+            hi[a] = min(max(hi[a], o[a]), o[a] + d[a] - 1) - o[a];
+        }
+        const int cap = P.nbr_cap;
+        const int64_t stride = P.nbr_stride;
+        if (lo[2] <= hi[2]) {
+            for (int cx = lo[0]; cx <= hi[0]; cx++) {
+                for (int cy = lo[1]; cy <= hi[1]; cy++) {
+                    uint32_t row = ((uint32_t)cx * (uint32_t)P.ny + (uint32_t)cy) * (uint32_t)P.nz;
+                    uint32_t beg = cell_start[row + lo[2]];
+                    uint32_t end = cell_start[row + hi[2] + 1];
+                    for (uint32_t q = beg; q < end; q++) {
+                        V3 dq = xi - v3(pos[q]);
+                        if (sqmag(dq) <= P.h2) {
+                            if (c < cap) nbr[(int64_t)c * stride + i] = (int32_t)q;
+                            c++;
+                        }
+                    }
+                }
+            }
+        }
+        count[i] = c;
+    }
+    // Overflow flag and the step's maximum count: one atomic per warp.
+    uint32_t m = (uint32_t)c;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0 && m > 0) {
+        atomicMax(&st->max_neighbors, m);
+        if (m > (uint32_t)P.nbr_cap) atomicOr(&st->error_flags, kErrNeighborOverflow);
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+void launch_grid_build(const GridBuildArgs& a, cudaStream_t s)
+{
+    const int T = 256;
+    const DevParams& P = a.P;
+    if (P.n > 0)
+        k_keys_hist<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.hist, a.status);
+    const int64_t n = (int64_t)P.cells + 1;
+    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
+    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
+    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
+    if (P.n > 0) {
+        k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
+        k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
+                                                       a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
+                                                       a.old_out, a.slot_of_id, a.sorted_key, a.status);
+        k_neighbors<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
+    }
+}
+
+}  // namespace lsp

@@ -1,0 +1,208 @@
+// Device-side types and per-particle arithmetic shared by all kernels.
+//
+// All translation units of liblsp are compiled with -fmad=false -prec-div=true
+// -prec-sqrt=true -ftz=false: every +, -, *, / and sqrtf below rounds once, IEEE
+// round-to-nearest, in source order. The per-particle expressions restate the
+// reference's CPU solver operation by operation (citations at each function), so
+// each particle's result matches the reference's bits when the neighbour sums are
+// taken in the same order, which the grid build guarantees.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lsp {
+
+constexpr int kTableSize = 1001;        // SPHKernel m_subdivision = 1000 (SPHKernel.cpp:4-7)
+constexpr int kMaxColliders = 64;
+constexpr int kMaxIterationsCap = 1024;
+
+// Error bits of DevStatus::error_flags.
+constexpr uint32_t kErrNaN = 1u;             // non-finite position or density
+constexpr uint32_t kErrNeighborOverflow = 2u; // a neighbour list exceeded its capacity
+constexpr uint32_t kErrTimeout = 4u;         // a bounded grid barrier gave up
+constexpr uint32_t kErrScan = 8u;            // the cell scan saw inconsistent counts
+
+struct Collider {
+    int sphere;     // 0 box, 1 sphere
+    int boundary;   // 0 obstacle (keep out), 1 boundary (keep in)
+    float cx, cy, cz;
+    float hx, hy, hz;   // box half extents
+    float radius;       // sphere radius
+    float pad;
+};
+
+struct DevStatus {
+    uint32_t error_flags;
+    uint32_t escaped;
+    uint32_t max_neighbors;
+    uint32_t max_err_bits;      // float bits of the current iteration's max |density error|
+    int32_t iterations;
+    int32_t converged;
+    int32_t warm_used;
+    uint32_t barrier_count;     // grid barrier arrivals (persistent loop)
+    uint32_t barrier_gen;
+    uint32_t timeout_site;
+    float last_ratio;
+    uint32_t pad[5];
+};
+
+struct DevParams {
+    float gx, gy, gz;
+    float h;            // kernel radius = grid spacing
+    float h2;           // h * h, the neighbour-test bound (SPHSpatialGrid.cpp:69)
+    float step;         // table division step h / 1000 (SPHKernel.cpp:134-137)
+    float radius;       // particle radius (collisions)
+    float mass;
+    float rho0;
+    float stiffness;
+    float neg;          // negative pressure factor
+    float viscosity;
+    float sigma;
+    float sigma_thr;
+    float restitution;
+    float friction;
+    float delta;        // PCISPH pressure scaling of this step
+    float eta;
+    float dt;
+    int n;
+    int keep_initial_velocity;
+    int ncoll;
+    int ox, oy, oz;     // grid origin in cell coordinates
+    int nx, ny, nz;     // grid dimensions
+    uint32_t cells;
+    int nbr_cap;        // neighbour list capacity per particle
+    int64_t nbr_stride; // column stride of the neighbour list (>= n)
+    int min_it, max_it;
+};
+
+// ----------------------------------------------------------------- vector ops
+// Vector3D semantics (LiquidPhysics/src/Math/Vector3D.cpp): component-wise, in order.
+struct V3 {
+    float x, y, z;
+};
+__device__ __forceinline__ V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+__device__ __forceinline__ V3 v3(const float4& a) { return V3{a.x, a.y, a.z}; }
+__device__ __forceinline__ V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ V3 operator*(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ V3 operator/(V3 a, float s) { return V3{a.x / s, a.y / s, a.z / s}; }
+__device__ __forceinline__ void operator+=(V3& a, V3 b) { a.x = a.x + b.x; a.y = a.y + b.y; a.z = a.z + b.z; }
+__device__ __forceinline__ void operator*=(V3& a, float s) { a.x = a.x * s; a.y = a.y * s; a.z = a.z * s; }
+// Vector3D::operator*(Vector3D) is a dot product (Vector3D.cpp:133-136).
+__device__ __forceinline__ float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// Vector3D::squareMagnitude / magnitude (Vector3D.cpp:55-63).
+__device__ __forceinline__ float sqmag(V3 a) { return a.x * a.x + a.y * a.y + a.z * a.z; }
+__device__ __forceinline__ float mag(V3 a) { return sqrtf(a.x * a.x + a.y * a.y + a.z * a.z); }
+// Vector3D::normalize (Vector3D.cpp:66-71): scale by the rounded reciprocal.
+__device__ __forceinline__ void normalize(V3& a)
+{
+    float m = mag(a);
+    if (m > 0.f) a *= (1.f / m);
+}
+__device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+// SPHKernel::get*Weight (SPHKernel.cpp:13-44): zero at or beyond h, else the table
+// entry at trunc(d / step).
+__device__ __forceinline__ float lookup(const float* tab, float d, const DevParams& P)
+{
+    if (d >= P.h) return 0.f;
+    int key = (int)(d / P.step);
+    return tab[key];
+}
+
+// ----------------------------------------------------------------- collisions
+// StaticCollisionObject::resolveCollisionWithParticle (StaticCollisionObject.cpp:21-38).
+__device__ __forceinline__ void resolve(V3& pos, V3& vel, V3 n, V3 point, const DevParams& P)
+{
+    float sep = dot(vel, n);
+    if (sep < 0.f) {
+        V3 vn = n * sep;
+        V3 vt = vel - vn;
+        vn *= -P.restitution;
+        vt *= P.friction;
+        vel = vn + vt;
+    }
+    pos = point;
+}
+
+// StaticCollisionBox (StaticCollisionBox.cpp:10-118) and StaticCollisionSphere
+// (StaticCollisionSphere.cpp:10-56) detection, then resolve on contact.
+__device__ __forceinline__ void collide(const Collider& o, V3& pos, V3& vel, const DevParams& P)
+{
+    const float r = P.radius;
+    V3 c = v3(o.cx, o.cy, o.cz);
+    V3 n = v3(0.f, 0.f, 0.f);
+    V3 point = pos;
+    bool found = false;
+    if (!o.sphere) {
+        V3 half = v3(o.hx, o.hy, o.hz);
+        V3 dv = c - pos;
+        V3 dist = v3(fabsf(dv.x), fabsf(dv.y), fabsf(dv.z));
+        if (!o.boundary) {
+            V3 pen = half - dist;
+            pen = v3(pen.x + r, pen.y + r, pen.z + r);
+            if (pen.x > 0.f && pen.y > 0.f && pen.z > 0.f) {
+                found = true;
+                if (pen.x <= pen.y && pen.x <= pen.z) {
+                    n.x = (pos.x - c.x >= 0.f) ? 1.f : -1.f;
+                    point.x = c.x + n.x * (half.x + r);
+                } else if (pen.y <= pen.x && pen.y <= pen.z) {
+                    n.y = (pos.y - c.y >= 0.f) ? 1.f : -1.f;
+                    point.y = c.y + n.y * (half.y + r);
+                } else if (pen.z <= pen.y && pen.z <= pen.x) {
+                    n.z = (pos.z - c.z >= 0.f) ? 1.f : -1.f;
+                    point.z = c.z + n.z * (half.z + r);
+                }
+            }
+        } else {
+            V3 pen = dist - half;
+            pen = v3(pen.x + r, pen.y + r, pen.z + r);
+            if (pen.x > 0.f || pen.y > 0.f || pen.z > 0.f) {
+                found = true;
+                if (pen.x > 0.f) {
+                    n.x = (pos.x - c.x <= 0.f) ? 1.f : -1.f;
+                    point.x = c.x - n.x * (half.x - r);
+                }
+                if (pen.y > 0.f) {
+                    n.y = (pos.y - c.y <= 0.f) ? 1.f : -1.f;
+                    point.y = c.y - n.y * (half.y - r);
+                }
+                if (pen.z > 0.f) {
+                    n.z = (pos.z - c.z <= 0.f) ? 1.f : -1.f;
+                    point.z = c.z - n.z * (half.z - r);
+                }
+                normalize(n);
+            }
+        }
+    } else {
+        float R = o.radius;
+        float dist = mag(c - pos);
+        float pen = o.boundary ? dist - (R - r) : (R + r) - dist;
+        if (pen > 0.f) {
+            found = true;
+            // Contact point from the un-normalised normal (StaticCollisionSphere.cpp:44-50).
+            if (!o.boundary) {
+                n = pos - c;
+                point = c + n * (R + r);
+            } else {
+                n = c - pos;
+                point = c - n * (R - r);
+            }
+            normalize(n);
+        }
+    }
+    if (found) resolve(pos, vel, n, point, P);
+}
+
+__device__ __forceinline__ void collide_all(const Collider* cols, int ncoll, V3& pos, V3& vel, const DevParams& P)
+{
+    for (int c = 0; c < ncoll; c++) collide(cols[c], pos, vel, P);
+}
+
+// Cell coordinate of the reference's CPU grid (SPHSpatialGrid.cpp:80-82).
+__device__ __forceinline__ int cell_coord(float x, float h) { return (int)(x / h); }
+
+__device__ __forceinline__ int id_of(const float4& p) { return __float_as_int(p.w); }
+
+}  // namespace lsp

@@ -1,0 +1,285 @@
+"""Python mirror of the reference solver API over the C ABI (liblsp.so).
+
+``SPHSolver`` and ``PCISPHSolver`` keep the method set of LiquidPhysics'
+``LiPhEn::SPHSolver`` (LiquidPhysics/include/SPHSolver.h:25-168) and
+``LiPhEn::PCISPHSolver`` (PCISPHSolver.h:7-44) in snake_case: scene setup
+(particles, static collision boxes/spheres), parameter setters/getters, one
+``update(dt)`` per step (PhysicSolver::update, PhysicSolver.h:10) and particle
+read-back. Arrays are numpy, in caller order. There is no CPU fallback: without
+``liblsp.so`` or a B200 the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, byref, c_float, c_int32, c_int64, c_uint32
+
+import numpy as np
+
+from . import abi
+
+_fp = POINTER(c_float)
+
+
+def _f32(a, shape_last=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a
+
+
+def _ptr(a, typ=_fp):
+    return a.ctypes.data_as(typ) if a is not None else None
+
+
+class SPHSolver:
+    """LiPhEn::SPHSolver on the GPU (ParallelizationType extended with CUDA)."""
+
+    SOLVER = abi.LSP_SOLVER_SPH
+
+    def __init__(self, params: abi.LspParams | None = None, device: int = -1, **overrides):
+        self._lib = abi.load_library()
+        p = params if params is not None else abi.default_params()
+        p = abi.default_params(**{**abi.params_dict(p), **overrides})
+        p.solver = self.SOLVER
+        h = ctypes.c_void_p()
+        abi.check(self._lib, self._lib.lsp_create(byref(p), device, byref(h)))
+        self._h = h
+        self._colliders = []
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.lsp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _call(self, name, *args):
+        return abi.check(self._lib, getattr(self._lib, name)(self._h, *args))
+
+    # ------------------------------------------------------------ parameters
+    @property
+    def params(self) -> abi.LspParams:
+        p = abi.LspParams()
+        self._call("lsp_get_params", byref(p))
+        return p
+
+    def set_params(self, **fields):
+        p = self.params
+        for k, v in fields.items():
+            if k == "gravity":
+                p.gravity[:] = tuple(v)
+            else:
+                setattr(p, k, v)
+        self._call("lsp_set_params", byref(p))
+
+    # Setters / getters of SPHSolver.h:79-109.
+    def set_gravity(self, g): self.set_params(gravity=g)
+    def set_particle_radius(self, r): self.set_params(particle_radius=r)
+    def set_kernel_radius_factor(self, f): self.set_params(kernel_radius_factor=f)
+    def set_rest_density(self, rho0): self.set_params(rest_density=rho0)
+    def set_viscosity_coefficient(self, mu): self.set_params(viscosity=mu)
+    def set_pressure_stiffness_coefficient(self, k): self.set_params(stiffness=k)
+    def set_negative_pressure_factor(self, f): self.set_params(negative_pressure_factor=f)
+    def set_surface_tension_coefficient(self, s): self.set_params(surface_tension=s)
+    def set_surface_tension_threshold(self, t): self.set_params(surface_tension_threshold=t)
+    def set_restitution_coefficient(self, e): self.set_params(restitution=e)
+    def set_friction_coefficient(self, f): self.set_params(friction=f)
+
+    def set_has_collision_object_data_changed(self, changed: bool = True):
+        """Colliders are re-uploaded whenever changed through this API; kept for parity."""
+
+    def get_gravity(self): return tuple(self.params.gravity)
+    def get_particle_radius(self): return self.params.particle_radius
+    def get_kernel_radius_factor(self): return self.params.kernel_radius_factor
+    def get_rest_density(self): return self.params.rest_density
+    def get_viscosity_coefficient(self): return self.params.viscosity
+    def get_pressure_stiffness_coefficient(self): return self.params.stiffness
+    def get_negative_pressure_factor(self): return self.params.negative_pressure_factor
+    def get_surface_tension_coefficient(self): return self.params.surface_tension
+    def get_surface_tension_threshold(self): return self.params.surface_tension_threshold
+    def get_restitution_coefficient(self): return self.params.restitution
+    def get_friction_coefficient(self): return self.params.friction
+
+    def get_particle_mass(self) -> float:
+        m = c_float()
+        self._call("lsp_particle_mass", byref(m))
+        return m.value
+
+    def get_kernel_radius(self) -> float:
+        h = c_float()
+        self._call("lsp_kernel_radius", byref(h))
+        return h.value
+
+    def get_particle_count(self) -> int:
+        n = c_int64()
+        self._call("lsp_particle_count", byref(n))
+        return n.value
+
+    def kernel_tables(self) -> np.ndarray:
+        out = np.empty(5 * abi.TABLE_SIZE, np.float32)
+        self._call("lsp_kernel_tables", _ptr(out), out.size)
+        return out.reshape(5, abi.TABLE_SIZE)
+
+    # ------------------------------------------------------------ scene
+    def add_particles(self, positions, velocities=None):
+        """SPHSolver::addParticle for each row (SPHSolver.cpp:129-135)."""
+        pos = _f32(positions).reshape(-1, 3)
+        vel = None if velocities is None else _f32(velocities).reshape(-1, 3)
+        if vel is not None and vel.shape != pos.shape:
+            raise ValueError("velocities must match positions")
+        self._call("lsp_add_particles", _ptr(pos), _ptr(vel), pos.shape[0])
+
+    def add_particle(self, position, velocity=None):
+        self.add_particles(np.asarray(position, np.float32)[None, :],
+                           None if velocity is None else np.asarray(velocity, np.float32)[None, :])
+
+    def remove_particles(self):
+        self._call("lsp_remove_particles")
+
+    def add_static_collision_box(self, center, half_extent, boundary: bool = False) -> int:
+        c = _f32(center)
+        h = _f32(half_extent)
+        self._call("lsp_add_box", _ptr(c), _ptr(h), abi.LSP_BOUNDARY if boundary else abi.LSP_OBSTACLE)
+        self._colliders.append("box")
+        return len(self._colliders) - 1
+
+    def add_static_collision_sphere(self, center, radius: float, boundary: bool = False) -> int:
+        c = _f32(center)
+        self._call("lsp_add_sphere", _ptr(c), float(radius), abi.LSP_BOUNDARY if boundary else abi.LSP_OBSTACLE)
+        self._colliders.append("sphere")
+        return len(self._colliders) - 1
+
+    def add_static_collision_object(self, collider) -> int:
+        """Takes a scenes.Collider (kind 'box' or 'sphere')."""
+        if collider.kind == "box":
+            return self.add_static_collision_box(collider.center, collider.size, collider.boundary)
+        return self.add_static_collision_sphere(collider.center, collider.size, collider.boundary)
+
+    def update_static_collision_box(self, index, center, half_extent):
+        self._call("lsp_update_box", int(index), _ptr(_f32(center)), _ptr(_f32(half_extent)))
+
+    def update_static_collision_sphere(self, index, center, radius):
+        self._call("lsp_update_sphere", int(index), _ptr(_f32(center)), float(radius))
+
+    def remove_static_collision_objects(self):
+        self._call("lsp_remove_colliders")
+        self._colliders = []
+
+    def clean_up(self):
+        """SPHSolver::cleanUp (SPHSolver.cpp:180-184)."""
+        self.remove_particles()
+        self.remove_static_collision_objects()
+
+    def set_domain(self, lo, hi):
+        self._call("lsp_set_domain", _ptr(_f32(lo)), _ptr(_f32(hi)))
+
+    # ------------------------------------------------------------ stepping
+    def update(self, dt: float) -> abi.LspStepStats:
+        """PhysicSolver::update (PhysicSolver.cpp:12-21)."""
+        st = abi.LspStepStats()
+        self._call("lsp_step", c_float(dt), byref(st))
+        return st
+
+    def step_many(self, dt: float, steps: int) -> abi.LspStepStats:
+        st = abi.LspStepStats()
+        self._call("lsp_step_many", c_float(dt), int(steps), byref(st))
+        return st
+
+    def synchronize(self):
+        self._call("lsp_synchronize")
+
+    # ------------------------------------------------------------ read-back
+    def read(self, field: int) -> np.ndarray:
+        n = self.get_particle_count()
+        shape = (n, 3) if field in abi.VECTOR_FIELDS else (n,)
+        out = np.empty(shape, np.float32)
+        self._call("lsp_read_field", int(field), _ptr(out), n)
+        return out
+
+    def positions(self) -> np.ndarray:
+        return self.read(abi.FIELD_POSITION)
+
+    def velocities(self) -> np.ndarray:
+        return self.read(abi.FIELD_VELOCITY)
+
+    def read_state(self):
+        n = self.get_particle_count()
+        x, v, h, o = (np.empty((n, 3), np.float32) for _ in range(4))
+        first = np.empty(n, np.int32)
+        self._call("lsp_read_state", _ptr(x), _ptr(v), _ptr(h), _ptr(o), _ptr(first, POINTER(c_int32)), n)
+        return x, v, h, o, first
+
+    def write_state(self, x, v, half, old_half, first):
+        n = self.get_particle_count()
+        arrs = [_f32(a).reshape(n, 3) for a in (x, v, half, old_half)]
+        f = np.ascontiguousarray(first, np.int32).reshape(n)
+        self._call("lsp_write_state", *(_ptr(a) for a in arrs), _ptr(f, POINTER(c_int32)), n)
+
+    def neighbors(self):
+        """Start-of-step neighbour lists of the last step: (offsets[n+1], caller ids)."""
+        n = self.get_particle_count()
+        off = np.empty(n + 1, np.int64)
+        self._call("lsp_read_neighbors", _ptr(off, POINTER(c_int64)), None, n, 0)
+        idx = np.empty(max(int(off[-1]), 1), np.int32)
+        self._call("lsp_read_neighbors", _ptr(off, POINTER(c_int64)), _ptr(idx, POINTER(c_int32)), n, idx.size)
+        return off, idx[: int(off[-1])]
+
+    def grid(self):
+        """(dims, origin, sorted keys, sorted caller ids, dense cell table) of the last step."""
+        n = self.get_particle_count()
+        dims = np.empty(3, np.int32)
+        org = np.empty(3, np.int32)
+        cells = c_int64()
+        self._call("lsp_grid_info", _ptr(dims, POINTER(c_int32)), _ptr(org, POINTER(c_int32)), byref(cells))
+        keys = np.empty(max(n, 1), np.uint32)
+        ids = np.empty(max(n, 1), np.int32)
+        start = np.empty(cells.value + 1, np.uint32)
+        self._call("lsp_read_grid", _ptr(keys, POINTER(c_uint32)), _ptr(ids, POINTER(c_int32)), n,
+                   _ptr(start, POINTER(c_uint32)), cells.value + 1)
+        return dims, org, keys[:n], ids[:n], start
+
+
+class PCISPHSolver(SPHSolver):
+    """LiPhEn::PCISPHSolver on the GPU."""
+
+    SOLVER = abi.LSP_SOLVER_PCISPH
+
+    def set_min_iterations(self, n: int):
+        """PCISPHSolver::setMinIterations (PCISPHSolver.cpp:342-345). The reference's loop runs
+        at most this many iterations (PCISPHSolver.cpp:64), so it sets pci_max_iterations."""
+        self.set_params(pci_max_iterations=int(n))
+
+    def get_min_iterations(self) -> int:
+        return self.params.pci_max_iterations
+
+    def set_max_density_error_ratio(self, eta: float):
+        self.set_params(pci_eta=float(eta))
+
+    def get_max_density_error_ratio(self) -> float:
+        return self.params.pci_eta
+
+    def set_minimum_iteration_floor(self, n: int):
+        """Extension: no convergence exit before n iterations (the reference has none)."""
+        self.set_params(pci_min_iterations=int(n))
+
+
+def from_scene(scene, device: int = -1) -> SPHSolver:
+    """Builds a solver for a scenes.Scene: parameters, particles, colliders, grid box."""
+    cls = PCISPHSolver if scene.params.solver == abi.LSP_SOLVER_PCISPH else SPHSolver
+    s = cls(scene.params, device=device)
+    if scene.domain is not None:
+        s.set_domain(*scene.domain)
+    if scene.n:
+        s.add_particles(scene.positions, scene.velocities)
+    for c in scene.colliders:
+        s.add_static_collision_object(c)
+    return s

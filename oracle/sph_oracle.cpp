@@ -1,0 +1,745 @@
+// Test infrastructure (the oracle), not product code. See sph_oracle.h.
+//
+// Every function restates a reference function and names it. In the FP32
+// instantiation each expression keeps the reference's operand order and rounding
+// points (compiled with -ffp-contract=off, as the reference must be for these
+// results to be reproducible), which is what makes bit-exact comparison with the
+// compiled reference (oracle/_ref) possible. Per-particle loops run in parallel
+// with OpenMP; each particle's result depends only on its own sums, taken in the
+// reference's neighbour order, so the thread count never changes a bit.
+#include "sph_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+template <typename T>
+struct V3 {
+	T x, y, z;
+	V3() : x(0), y(0), z(0) {}
+	V3(T a, T b, T c) : x(a), y(b), z(c) {}
+	V3 operator+(const V3& o) const { return V3(x + o.x, y + o.y, z + o.z); }
+	V3 operator-(const V3& o) const { return V3(x - o.x, y - o.y, z - o.z); }
+	V3 operator*(T s) const { return V3(x * s, y * s, z * s); }
+	V3 operator/(T s) const { return V3(x / s, y / s, z / s); }
+	void operator+=(const V3& o) { x += o.x; y += o.y; z += o.z; }
+	void operator*=(T s) { x *= s; y *= s; z *= s; }
+	// Vector3D::operator*(const Vector3D&) is the dot product (Vector3D.cpp:133-136).
+	T dot(const V3& o) const { return x * o.x + y * o.y + z * o.z; }
+	// Vector3D::magnitude / squareMagnitude (Vector3D.cpp:55-63).
+	T sq() const { return x * x + y * y + z * z; }
+	T mag() const { return std::sqrt(x * x + y * y + z * z); }
+	// Vector3D::normalize (Vector3D.cpp:66-71): multiply by the rounded reciprocal.
+	void normalize() { T m = mag(); if (m > 0) { *this *= ((T)1 / m); } }
+	V3 absv() const { return V3(std::fabs(x), std::fabs(y), std::fabs(z)); }
+	V3 addScalar(T s) const { return V3(x + s, y + s, z + s); }
+};
+
+// Lookup-table kernels: SPHKernel.cpp:13-44 (lookup), :93-104 (radius powers),
+// :113-137 (tables); coefficients and formulas of DefaultKernel.cpp:12-42 (poly6),
+// PressureKernel.cpp:12-42 (spiky), ViscosityKernel.cpp:12-40. The coefficients are
+// formed in double (M_PI is double) and rounded to T, as in the reference.
+template <typename T>
+struct Tables {
+	static constexpr int kSub = 1000;
+	T radius = 0, r2 = 0, r3 = 0, r4 = 0, r5 = 0, r6 = 0, r9 = 0, step = 0;
+	std::vector<T> w, dw, d2w, spiky_dw, visc_d2w;
+
+	void build(T h)
+	{
+		radius = h;
+		r2 = radius * radius; r3 = r2 * radius; r4 = r3 * radius; r5 = r4 * radius;
+		r6 = r5 * radius; r9 = r6 * r3;
+		step = radius / kSub;
+		const double pi = 3.14159265358979323846;
+		T poly_k = (T)(315.0 / (64.0 * pi * (double)r9));
+		T poly_d1 = (T)(-945.0 / (32.0 * pi * (double)r9));
+		T poly_d2 = (T)(-945.0 / (32.0 * pi * (double)r9));
+		T spiky_d1 = (T)(-45.0 / (pi * (double)r6));
+		T visc_d2 = (T)(45.0 / (pi * (double)r6));
+		w.resize(kSub + 1); dw.resize(kSub + 1); d2w.resize(kSub + 1);
+		spiky_dw.resize(kSub + 1); visc_d2w.resize(kSub + 1);
+		for (int i = 0; i <= kSub; i++)
+		{
+			T d = i * step;
+			T t = r2 - d * d;
+			w[i] = poly_k * t * t * t;
+			dw[i] = poly_d1 * t * t;
+			d2w[i] = poly_d2 * (r2 - d * d) * (3 * r2 - 7 * d * d);
+			T s = radius - d;
+			spiky_dw[i] = spiky_d1 * s * s;
+			visc_d2w[i] = visc_d2 * (radius - d);
+		}
+	}
+	// SPHKernel::get*Weight: zero at or beyond the radius, else the entry at trunc(d/step).
+	T look(const std::vector<T>& tab, T d) const
+	{
+		if (d >= radius) return 0;
+		int key = (int)(d / step);
+		return tab[key];
+	}
+};
+
+struct Collider {
+	bool sphere;
+	bool boundary;
+	float c[3];
+	float half[3];
+	float radius;
+};
+
+template <typename T>
+struct CollisionData { V3<T> position, velocity; T radius, restitution, friction; };
+
+// StaticCollisionObject::resolveCollisionWithParticle (StaticCollisionObject.cpp:21-38).
+template <typename T>
+void resolve(CollisionData<T>& d, const V3<T>& n, const V3<T>& point)
+{
+	T sep = d.velocity.dot(n);
+	if (sep < 0)
+	{
+		V3<T> vn = n * sep;
+		V3<T> vt = d.velocity - vn;
+		vn *= -d.restitution;
+		vt *= d.friction;
+		d.velocity = vn + vt;
+	}
+	d.position = point;
+}
+
+// StaticCollisionBox::detectCollisionWithParticle / calcPenetration / calcCollisionInfo
+// (StaticCollisionBox.cpp:10-118) and StaticCollisionSphere::* (StaticCollisionSphere.cpp:10-56),
+// followed by resolve when a collision is found (StaticCollisionObject.cpp:10-19).
+template <typename T>
+void collide(const Collider& o, CollisionData<T>& d)
+{
+	V3<T> c((T)o.c[0], (T)o.c[1], (T)o.c[2]);
+	V3<T> n;
+	V3<T> point = d.position;
+	bool found = false;
+	if (!o.sphere)
+	{
+		V3<T> half((T)o.half[0], (T)o.half[1], (T)o.half[2]);
+		V3<T> dist = (c - d.position).absv();
+		V3<T> pen = o.boundary ? (dist - half).addScalar(d.radius) : (half - dist).addScalar(d.radius);
+		if (!o.boundary)
+		{
+			if (pen.x > 0 && pen.y > 0 && pen.z > 0)
+			{
+				found = true;
+				if (pen.x <= pen.y && pen.x <= pen.z)
+				{
+					n.x = (d.position.x - c.x >= 0) ? (T)1 : (T)-1;
+					point.x = c.x + n.x * (half.x + d.radius);
+				}
+				else if (pen.y <= pen.x && pen.y <= pen.z)
+				{
+					n.y = (d.position.y - c.y >= 0) ? (T)1 : (T)-1;
+					point.y = c.y + n.y * (half.y + d.radius);
+				}
+				else if (pen.z <= pen.y && pen.z <= pen.x)
+				{
+					n.z = (d.position.z - c.z >= 0) ? (T)1 : (T)-1;
+					point.z = c.z + n.z * (half.z + d.radius);
+				}
+			}
+		}
+		else
+		{
+			if (pen.x > 0 || pen.y > 0 || pen.z > 0)
+			{
+				found = true;
+				if (pen.x > 0)
+				{
+					n.x = (d.position.x - c.x <= 0) ? (T)1 : (T)-1;
+					point.x = c.x - n.x * (half.x - d.radius);
+				}
+				if (pen.y > 0)
+				{
+					n.y = (d.position.y - c.y <= 0) ? (T)1 : (T)-1;
+					point.y = c.y - n.y * (half.y - d.radius);
+				}
+				if (pen.z > 0)
+				{
+					n.z = (d.position.z - c.z <= 0) ? (T)1 : (T)-1;
+					point.z = c.z - n.z * (half.z - d.radius);
+				}
+				n.normalize();
+			}
+		}
+	}
+	else
+	{
+		T R = (T)o.radius;
+		T dist = (c - d.position).mag();
+		T pen = o.boundary ? dist - (R - d.radius) : (R + d.radius) - dist;
+		if (pen > 0)
+		{
+			found = true;
+			// The contact point uses the un-normalised normal (StaticCollisionSphere.cpp:44-50).
+			if (!o.boundary)
+			{
+				n = d.position - c;
+				point = c + n * (R + d.radius);
+			}
+			else
+			{
+				n = c - d.position;
+				point = c - n * (R - d.radius);
+			}
+			n.normalize();
+		}
+	}
+	if (found) resolve(d, n, point);
+}
+
+struct SimBase {
+	virtual ~SimBase() {}
+	lsp_params p{};
+	std::vector<Collider> colliders;
+	std::vector<int64_t> nbrOffsets;
+	std::vector<int32_t> nbrIndex;
+	virtual int64_t count() const = 0;
+	virtual void add(const float* xyz, const float* vel, int64_t n) = 0;
+	virtual int step(float dt, lsp_step_stats* st) = 0;
+	virtual int get(int field, float* out) = 0;
+	virtual int getd(int field, double* out) = 0;
+	virtual void setState(const float*, const float*, const float*, const float*, const int32_t*) = 0;
+	virtual void configure() = 0;
+	virtual float mass() const = 0;
+	virtual float kernelRadius() const = 0;
+	virtual float delta(float dt) const = 0;
+	virtual void tables(float* out) const = 0;
+};
+
+template <typename T>
+struct Sim : SimBase {
+	Tables<T> tab;
+	T h = 0, m = 0;
+	std::vector<V3<T>> x, v, half, oldHalf, F, px, phalf, pF;
+	std::vector<T> rho, pres, prho, err;
+	std::vector<uint8_t> first;
+
+	int64_t count() const override { return (int64_t)x.size(); }
+	float mass() const override { return (float)m; }
+	float kernelRadius() const override { return (float)h; }
+
+	// SPHSolver::recalcKernelRadius (SPHSolver.cpp:509-523) and recalcParticleMass (:480-507).
+	void configure() override
+	{
+		h = (T)p.kernel_radius_factor * (T)p.particle_radius;
+		tab.build(h);
+		T stepSize = (T)1.6f * (T)p.particle_radius;
+		T sum = 0;
+		for (int i = -3; i <= 3; i++)
+			for (int j = -3; j <= 3; j++)
+				for (int k = -3; k <= 3; k++)
+				{
+					V3<T> q(i * stepSize, j * stepSize, k * stepSize);
+					sum += tab.look(tab.w, q.mag());
+				}
+		m = (T)p.rest_density / sum;
+		if (p.mass_override > 0) m = (T)p.mass_override;
+	}
+
+	// PCISPHSolver::calcDelta (PCISPHSolver.cpp:286-328).
+	T calcDelta(T dt) const
+	{
+		T stepSize = (T)1.6f * (T)p.particle_radius;
+		V3<T> d1;
+		T d2 = 0;
+		for (int i = -3; i <= 3; i++)
+			for (int j = -3; j <= 3; j++)
+				for (int k = -3; k <= 3; k++)
+				{
+					V3<T> q(i * stepSize, j * stepSize, k * stepSize);
+					T dist = q.mag();
+					if (dist > 0)
+					{
+						V3<T> dir = q / dist;
+						V3<T> g = dir * tab.look(tab.spiky_dw, dist);
+						d1 += g;
+						d2 += g.dot(g);
+					}
+				}
+		T denom = -(d1.dot(d1)) - d2;
+		T beta = dt * m / (T)p.rest_density;
+		beta = 2 * beta * beta;
+		T delta = 0;
+		if (std::fabs(denom) > 0) delta = -1 / (beta * denom);
+		return delta;
+	}
+	float delta(float dt) const override { return (float)calcDelta((T)dt); }
+
+	void tables(float* out) const override
+	{
+		const std::vector<T>* t[5] = {&tab.w, &tab.dw, &tab.d2w, &tab.spiky_dw, &tab.visc_d2w};
+		for (int k = 0; k < 5; k++)
+			for (int i = 0; i <= Tables<T>::kSub; i++) out[k * (Tables<T>::kSub + 1) + i] = (float)(*t[k])[i];
+	}
+
+	void add(const float* xyz, const float* vel, int64_t n) override
+	{
+		for (int64_t i = 0; i < n; i++)
+		{
+			x.push_back(V3<T>(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]));
+			v.push_back(vel ? V3<T>(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]) : V3<T>());
+			half.push_back(V3<T>()); oldHalf.push_back(V3<T>()); F.push_back(V3<T>());
+			px.push_back(V3<T>()); phalf.push_back(V3<T>()); pF.push_back(V3<T>());
+			rho.push_back(0); pres.push_back(0); prho.push_back(0); err.push_back(0);
+			first.push_back(1);
+		}
+	}
+
+	void setState(const float* xs, const float* vs, const float* hs, const float* os, const int32_t* fs) override
+	{
+		for (int64_t i = 0; i < count(); i++)
+		{
+			x[i] = V3<T>(xs[3 * i], xs[3 * i + 1], xs[3 * i + 2]);
+			v[i] = V3<T>(vs[3 * i], vs[3 * i + 1], vs[3 * i + 2]);
+			half[i] = V3<T>(hs[3 * i], hs[3 * i + 1], hs[3 * i + 2]);
+			oldHalf[i] = V3<T>(os[3 * i], os[3 * i + 1], os[3 * i + 2]);
+			first[i] = fs[i] != 0;
+			F[i] = V3<T>();
+		}
+	}
+
+	// SPHSpatialGrid::build / findNeighborParticles / calcHashValue (SPHSpatialGrid.cpp:19-90),
+	// called per particle by SPHSolver::buildCachedNeighborLists (SPHSolver.cpp:431-440).
+	// Lists include the particle itself and keep the reference's order: cells visited
+	// i (x) -> j (y) -> k (z) ascending, each hash bucket in insertion order.
+	void buildNeighborLists()
+	{
+		const int64_t N = count();
+		auto cellOf = [&](T c) { return (int)(c / h); };
+		auto hash = [](int i, int j, int k) { return 541 * i + 79 * j + 31 * k; };
+		std::unordered_map<int, std::vector<int32_t>> grid;
+		for (int64_t i = 0; i < N; i++)
+			grid[hash(cellOf(x[i].x), cellOf(x[i].y), cellOf(x[i].z))].push_back((int32_t)i);
+		std::vector<std::vector<int32_t>> lists(N);
+		const T r2 = h * h;
+#pragma omp parallel for schedule(dynamic, 256)
+		for (int64_t a = 0; a < N; a++)
+		{
+			const V3<T> q = x[a];
+			int iMin = (int)((q.x - h) / h), iMax = (int)((q.x + h) / h);
+			int jMin = (int)((q.y - h) / h), jMax = (int)((q.y + h) / h);
+			int kMin = (int)((q.z - h) / h), kMax = (int)((q.z + h) / h);
+			std::vector<int32_t>& out = lists[a];
+			for (int i = iMin; i <= iMax; i++)
+				for (int j = jMin; j <= jMax; j++)
+					for (int k = kMin; k <= kMax; k++)
+					{
+						auto it = grid.find(hash(i, j, k));
+						if (it == grid.end()) continue;
+						for (int32_t b : it->second)
+							if ((q - x[b]).sq() <= r2) out.push_back(b);
+					}
+		}
+		nbrOffsets.assign(N + 1, 0);
+		for (int64_t i = 0; i < N; i++) nbrOffsets[i + 1] = nbrOffsets[i] + (int64_t)lists[i].size();
+		nbrIndex.resize(nbrOffsets[N]);
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+			std::copy(lists[i].begin(), lists[i].end(), nbrIndex.begin() + nbrOffsets[i]);
+	}
+
+	// SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
+	void densityPressure()
+	{
+		const int64_t N = count();
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+		{
+			T sum = 0;
+			for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+				sum += tab.look(tab.w, (x[nbrIndex[e]] - x[i]).mag());
+			rho[i] = m * sum;
+			T pr = (T)p.stiffness * (rho[i] - (T)p.rest_density);
+			if (pr < 0) pr *= (T)p.negative_pressure_factor;
+			pres[i] = pr;
+		}
+	}
+
+	// SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248).
+	void nonPressureForces()
+	{
+		const int64_t N = count();
+		const V3<T> g((T)p.gravity[0], (T)p.gravity[1], (T)p.gravity[2]);
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+		{
+			F[i] += g * rho[i];
+			V3<T> normal;
+			for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+			{
+				int32_t j = nbrIndex[e];
+				V3<T> dir = x[i] - x[j];
+				T d = (x[j] - x[i]).mag();
+				normal += dir * tab.look(tab.dw, d) / rho[j];
+			}
+			normal *= m;
+			T len = normal.mag();
+			if (len > (T)p.surface_tension_threshold)
+			{
+				T lap = 0;
+				for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+				{
+					int32_t j = nbrIndex[e];
+					T d = (x[i] - x[j]).mag();
+					lap += tab.look(tab.d2w, d) / rho[j];
+				}
+				V3<T> st = (normal / len) * (-(T)p.surface_tension * lap * m);
+				F[i] += st;
+			}
+			V3<T> visc;
+			for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+			{
+				int32_t j = nbrIndex[e];
+				if (j == i) continue;
+				T d = (x[i] - x[j]).mag();
+				visc += ((v[j] - v[i]) / rho[j]) * tab.look(tab.visc_d2w, d);
+			}
+			visc *= (T)p.viscosity * m;
+			F[i] += visc;
+		}
+	}
+
+	// SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
+	void sphPressureForces()
+	{
+		const int64_t N = count();
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+		{
+			V3<T> pf;
+			T tf = pres[i] / (rho[i] * rho[i]);
+			for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+			{
+				int32_t j = nbrIndex[e];
+				if (j == i) continue;
+				T d = (x[i] - x[j]).mag();
+				V3<T> dir = (x[i] - x[j]) / d;
+				pf += dir * tab.look(tab.spiky_dw, d) * (tf + pres[j] / (rho[j] * rho[j]));
+			}
+			pf *= -(m * rho[i]);
+			F[i] += pf;
+		}
+	}
+
+	CollisionData<T> collisionData(const V3<T>& pos, const V3<T>& vel) const
+	{
+		CollisionData<T> d;
+		d.position = pos; d.velocity = vel;
+		d.radius = (T)p.particle_radius; d.restitution = (T)p.restitution; d.friction = (T)p.friction;
+		return d;
+	}
+
+	// PCISPHSolver::accumulatePressureForces, CPU branch (PCISPHSolver.cpp:50-170), with the
+	// optional minimum iteration count and the optional velocity keep (both off by default).
+	void pcisphPressureForces(T dt, lsp_step_stats* st)
+	{
+		const int64_t N = count();
+		const T delta = calcDelta(dt);
+		const T rho0 = (T)p.rest_density;
+		const T neg = (T)p.negative_pressure_factor;
+		for (int64_t i = 0; i < N; i++) { pres[i] = 0; pF[i] = V3<T>(); }
+		int maxIt = p.pci_max_iterations, minIt = p.pci_min_iterations;
+		int it = 0;
+		T ratio = 0;
+		bool converged = false;
+		for (int k = 0; k < maxIt; k++)
+		{
+			it = k + 1;
+			// Predict velocity and position (:67-81).
+#pragma omp parallel for schedule(static)
+			for (int64_t i = 0; i < N; i++)
+			{
+				V3<T> hv = half[i];
+				V3<T> acc = (F[i] + pF[i]) / rho[i];
+				if (first[i]) hv = v[i] - acc * dt / 2;
+				V3<T> ph = hv + acc * dt;
+				phalf[i] = ph;
+				px[i] = x[i] + ph * dt;
+			}
+			// Collisions on the prediction (:84-97); aproximateVelocity wipes v on a first step.
+#pragma omp parallel for schedule(static)
+			for (int64_t i = 0; i < N; i++)
+			{
+				CollisionData<T> d = collisionData(px[i], phalf[i]);
+				for (const Collider& o : colliders) collide(o, d);
+				px[i] = d.position;
+				phalf[i] = d.velocity;
+				if (!p.keep_initial_velocity) v[i] = (oldHalf[i] + half[i]) / 2;
+			}
+			// Predicted density, error, pressure (:100-126).
+#pragma omp parallel for schedule(static)
+			for (int64_t i = 0; i < N; i++)
+			{
+				T sum = 0;
+				for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+					sum += tab.look(tab.w, (px[nbrIndex[e]] - px[i]).mag());
+				T pd = m * sum;
+				T er = pd - rho0;
+				T pp = delta * er;
+				if (pp < 0) { er *= neg; pp *= neg; }
+				prho[i] = pd;
+				err[i] = er;
+				pres[i] = pres[i] + pp;
+			}
+			// Pressure force at the prediction (:129-150); prefactor uses the current density.
+#pragma omp parallel for schedule(static)
+			for (int64_t i = 0; i < N; i++)
+			{
+				V3<T> pf;
+				T tf = pres[i] / (prho[i] * prho[i]);
+				for (int64_t e = nbrOffsets[i]; e < nbrOffsets[i + 1]; e++)
+				{
+					int32_t j = nbrIndex[e];
+					if (j == i) continue;
+					T d = (px[j] - px[i]).mag();
+					V3<T> dir = (px[i] - px[j]) / d;
+					pf += dir * tab.look(tab.spiky_dw, d) * (tf + pres[j] / (prho[j] * prho[j]));
+				}
+				pf *= -(m * rho[i]);
+				if (std::isnan(pf.x)) pf = V3<T>();
+				pF[i] = pf;
+			}
+			// Max density error and the exit test (:152-162).
+			T maxErr = 0;
+			for (int64_t i = 0; i < N; i++) maxErr = std::max(maxErr, (T)std::fabs(err[i]));
+			ratio = maxErr / rho0;
+			converged = std::fabs(ratio) < (T)p.pci_eta;
+			if (converged && it >= minIt) break;
+		}
+		for (int64_t i = 0; i < N; i++) F[i] += pF[i];
+		if (st)
+		{
+			st->iterations = it;
+			st->converged = converged ? 1 : 0;
+			st->max_density_error_ratio = (double)ratio;
+		}
+	}
+
+	// SPHParticle::integrate (SPHParticle.cpp:30-44), per particle.
+	void integrate(T dt)
+	{
+		const int64_t N = count();
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+		{
+			V3<T> acc = F[i] / rho[i];
+			if (first[i]) { half[i] = v[i] - acc * dt / 2; first[i] = 0; }
+			oldHalf[i] = half[i];
+			half[i].x += acc.x * dt; half[i].y += acc.y * dt; half[i].z += acc.z * dt;
+			x[i].x += half[i].x * dt; x[i].y += half[i].y * dt; x[i].z += half[i].z * dt;
+			F[i] = V3<T>();
+		}
+	}
+
+	// SPHSolver::handleCollisions, CPU branch (SPHSolver.cpp:337-355).
+	void handleCollisions()
+	{
+		const int64_t N = count();
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < N; i++)
+		{
+			CollisionData<T> d = collisionData(x[i], half[i]);
+			for (const Collider& o : colliders) collide(o, d);
+			x[i] = d.position;
+			half[i] = d.velocity;
+			v[i] = (oldHalf[i] + half[i]) / 2;
+		}
+	}
+
+	// PhysicSolver::update (PhysicSolver.cpp:12-21) with SPHSolver's hooks.
+	int step(float dtf, lsp_step_stats* st) override
+	{
+		T dt = (T)dtf;
+		if (st) std::memset(st, 0, sizeof(*st));
+		buildNeighborLists();
+		densityPressure();
+		nonPressureForces();
+		if (p.solver == LSP_SOLVER_PCISPH) pcisphPressureForces(dt, st);
+		else sphPressureForces();
+		integrate(dt);
+		handleCollisions();
+		if (st)
+		{
+			int64_t mx = 0;
+			for (int64_t i = 0; i < count(); i++) mx = std::max(mx, nbrOffsets[i + 1] - nbrOffsets[i]);
+			st->max_neighbors = (int32_t)mx;
+			st->converged = p.solver == LSP_SOLVER_PCISPH ? st->converged : 1;
+		}
+		return 0;
+	}
+
+	template <typename O>
+	int getT(int field, O* out)
+	{
+		const int64_t N = count();
+		auto put = [&](const std::vector<V3<T>>& a) {
+			for (int64_t i = 0; i < N; i++) { out[3 * i] = (O)a[i].x; out[3 * i + 1] = (O)a[i].y; out[3 * i + 2] = (O)a[i].z; }
+		};
+		auto puts = [&](const std::vector<T>& a) { for (int64_t i = 0; i < N; i++) out[i] = (O)a[i]; };
+		switch (field)
+		{
+		case LSP_FIELD_POSITION: put(x); break;
+		case LSP_FIELD_VELOCITY: put(v); break;
+		case LSP_FIELD_HALF_VELOCITY: put(half); break;
+		case LSP_FIELD_OLD_HALF_VELOCITY: put(oldHalf); break;
+		case LSP_FIELD_DENSITY: puts(rho); break;
+		case LSP_FIELD_PRESSURE: puts(pres); break;
+		case LSP_FIELD_FIRST_STEP: for (int64_t i = 0; i < N; i++) out[i] = first[i] ? 1 : 0; break;
+		case LSP_FIELD_PRED_DENSITY: puts(prho); break;
+		case LSP_FIELD_DENSITY_ERROR: puts(err); break;
+		case LSP_FIELD_PRED_POSITION: put(px); break;
+		case LSP_FIELD_PRED_HALF_VELOCITY: put(phalf); break;
+		case LSP_FIELD_PRED_PRESSURE_FORCE: put(pF); break;
+		case LSP_FIELD_NEIGHBOR_COUNT:
+			if ((int64_t)nbrOffsets.size() != N + 1) return -1;
+			for (int64_t i = 0; i < N; i++) out[i] = (O)(nbrOffsets[i + 1] - nbrOffsets[i]);
+			break;
+		case LSP_FIELD_SPEED_SQUARED: for (int64_t i = 0; i < N; i++) out[i] = (O)v[i].sq(); break;
+		default: return -1;
+		}
+		return 0;
+	}
+	int get(int field, float* out) override { return getT(field, out); }
+	int getd(int field, double* out) override { return getT(field, out); }
+};
+
+}  // namespace
+
+extern "C" {
+
+void orc_set_threads(int threads) { if (threads > 0) omp_set_num_threads(threads); }
+
+void* orc_create(const lsp_params* p, int fp64)
+{
+	SimBase* s = fp64 ? (SimBase*)new Sim<double>() : (SimBase*)new Sim<float>();
+	s->p = *p;
+	s->configure();
+	return s;
+}
+
+void orc_destroy(void* h) { delete (SimBase*)h; }
+
+int orc_set_params(void* h, const lsp_params* p)
+{
+	SimBase* s = (SimBase*)h;
+	s->p = *p;
+	s->configure();
+	return 0;
+}
+
+int orc_add_particles(void* h, const float* xyz, const float* vel, int64_t n)
+{
+	((SimBase*)h)->add(xyz, vel, n);
+	return 0;
+}
+
+int orc_add_box(void* h, const float center[3], const float half_extent[3], int kind)
+{
+	Collider c{};
+	c.sphere = false; c.boundary = kind == LSP_BOUNDARY;
+	for (int a = 0; a < 3; a++) { c.c[a] = center[a]; c.half[a] = half_extent[a]; }
+	((SimBase*)h)->colliders.push_back(c);
+	return 0;
+}
+
+int orc_add_sphere(void* h, const float center[3], float radius, int kind)
+{
+	Collider c{};
+	c.sphere = true; c.boundary = kind == LSP_BOUNDARY; c.radius = radius;
+	for (int a = 0; a < 3; a++) c.c[a] = center[a];
+	((SimBase*)h)->colliders.push_back(c);
+	return 0;
+}
+
+int orc_update_box(void* h, int index, const float center[3], const float half_extent[3])
+{
+	SimBase* s = (SimBase*)h;
+	if (index < 0 || index >= (int)s->colliders.size() || s->colliders[index].sphere) return -1;
+	for (int a = 0; a < 3; a++) { s->colliders[index].c[a] = center[a]; s->colliders[index].half[a] = half_extent[a]; }
+	return 0;
+}
+
+int orc_update_sphere(void* h, int index, const float center[3], float radius)
+{
+	SimBase* s = (SimBase*)h;
+	if (index < 0 || index >= (int)s->colliders.size() || !s->colliders[index].sphere) return -1;
+	for (int a = 0; a < 3; a++) s->colliders[index].c[a] = center[a];
+	s->colliders[index].radius = radius;
+	return 0;
+}
+
+int64_t orc_count(void* h) { return ((SimBase*)h)->count(); }
+int orc_step(void* h, float dt, lsp_step_stats* st) { return ((SimBase*)h)->step(dt, st); }
+int orc_get(void* h, int field, float* out) { return ((SimBase*)h)->get(field, out); }
+int orc_get_f64(void* h, int field, double* out) { return ((SimBase*)h)->getd(field, out); }
+int orc_set_state(void* h, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first)
+{
+	((SimBase*)h)->setState(x, v, half, old_half, first);
+	return 0;
+}
+float orc_mass(void* h) { return ((SimBase*)h)->mass(); }
+float orc_kernel_radius(void* h) { return ((SimBase*)h)->kernelRadius(); }
+float orc_delta(void* h, float dt) { return ((SimBase*)h)->delta(dt); }
+void orc_tables(void* h, float* out) { ((SimBase*)h)->tables(out); }
+int64_t orc_neighbor_total(void* h) { SimBase* s = (SimBase*)h; return s->nbrOffsets.empty() ? 0 : s->nbrOffsets.back(); }
+void orc_neighbor_lists(void* h, int64_t* offsets, int32_t* index)
+{
+	SimBase* s = (SimBase*)h;
+	std::memcpy(offsets, s->nbrOffsets.data(), s->nbrOffsets.size() * sizeof(int64_t));
+	std::memcpy(index, s->nbrIndex.data(), s->nbrIndex.size() * sizeof(int32_t));
+}
+
+// Device grid-build specification. Cell coordinates are those of the reference's CPU grid,
+// c = (int)(x / h) per axis (SPHSpatialGrid.cpp:80-82), clamped into the grid box
+// [origin, origin + dims - 1] (a clamped particle is counted in *escaped). The cell key
+// orders cells as the reference's neighbour search visits them, x slowest and z fastest
+// (SPHSpatialGrid.cpp:51-57): key = ((cx - ox) * dims.y + (cy - oy)) * dims.z + (cz - oz).
+// Particles are ordered by (key, caller id), which is the bucket order of the CPU grid.
+// cell_start has cells + 1 entries: cell_start[g] = number of particles with key < g.
+int orc_grid_build(const float* xyz, int64_t n, float h, const int32_t origin[3], const int32_t dims[3],
+                   uint32_t* keys_sorted, int32_t* ids_sorted, uint32_t* cell_start, int64_t* escaped)
+{
+	const int64_t cells = (int64_t)dims[0] * dims[1] * dims[2];
+	std::vector<std::pair<uint32_t, int32_t>> kv(n);
+	int64_t esc = 0;
+	for (int64_t i = 0; i < n; i++)
+	{
+		int32_t c[3];
+		bool out = false;
+		for (int a = 0; a < 3; a++)
+		{
+			int v = (int)(xyz[3 * i + a] / h);
+			if (v < origin[a]) { v = origin[a]; out = true; }
+			if (v > origin[a] + dims[a] - 1) { v = origin[a] + dims[a] - 1; out = true; }
+			c[a] = v - origin[a];
+		}
+		esc += out ? 1 : 0;
+		uint32_t key = (uint32_t)(((int64_t)c[0] * dims[1] + c[1]) * dims[2] + c[2]);
+		kv[i] = {key, (int32_t)i};
+	}
+	std::sort(kv.begin(), kv.end());
+	std::vector<uint32_t> hist(cells + 1, 0);
+	for (int64_t i = 0; i < n; i++)
+	{
+		keys_sorted[i] = kv[i].first;
+		ids_sorted[i] = kv[i].second;
+		hist[kv[i].first]++;
+	}
+	uint32_t run = 0;
+	for (int64_t g = 0; g <= cells; g++) { cell_start[g] = run; run += hist[g]; }
+	if (escaped) *escaped = esc;
+	return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,127 @@
+"""The oracle pinned to the compiled reference CPU solver (no GPU needed).
+
+oracle/_ref/libref_sph.so is the reference's own LiquidPhysics/src, compiled
+unmodified (oracle/Makefile). oracle/liblsp_oracle.so is the project's restatement.
+They must agree bit for bit on every field, every step, and on the neighbour lists.
+"""
+import numpy as np
+import pytest
+
+from liquidsimulation_b200 import abi, scenes
+
+FIELDS = [abi.FIELD_POSITION, abi.FIELD_VELOCITY, abi.FIELD_HALF_VELOCITY, abi.FIELD_DENSITY,
+          abi.FIELD_PRESSURE, abi.FIELD_FIRST_STEP]
+PCI_FIELDS = [abi.FIELD_PRED_DENSITY, abi.FIELD_DENSITY_ERROR, abi.FIELD_PRED_POSITION,
+              abi.FIELD_PRED_HALF_VELOCITY, abi.FIELD_PRED_PRESSURE_FORCE]
+
+
+def same_bits(a, b):
+    return np.array_equal(np.asarray(a, np.float32).view(np.uint32), np.asarray(b, np.float32).view(np.uint32))
+
+
+@pytest.fixture
+def need_ref(ref_available):
+    if not ref_available:
+        pytest.skip("reference library not built (needs the reference sources)")
+
+
+def _scenes():
+    out = []
+    out.append(("pcisph_obstacles", scenes.small_box_scene(), 6))
+    out.append(("sph_obstacles", scenes.small_box_scene(solver=abi.LSP_SOLVER_SPH), 6))
+    out.append(("sph_dam_break_half", scenes.dam_break_sph(scale=0.5), 10))
+    sc = scenes.small_box_scene(negative_pressure_factor=0.5, surface_tension_threshold=0.5, surface_tension=0.4)
+    sc.colliders.append(scenes.Collider("sphere", (0.3, 0.3, 0.3), 0.45, True))
+    sc.velocities[:] = np.array([0.4, -0.1, 0.2], np.float32)
+    out.append(("pcisph_sphere_boundary_negp", sc, 6))
+    sc = scenes.small_box_scene(n_side=(9, 9, 9), pci_max_iterations=20, pci_eta=0.001)
+    out.append(("pcisph_tight_eta", sc, 4))
+    return out
+
+
+@pytest.mark.parametrize("name,scene,steps", _scenes(), ids=[s[0] for s in _scenes()])
+def test_restatement_matches_reference(oracle_mod, need_ref, name, scene, steps):
+    ref = oracle_mod.RefSolver(scene, capture_neighbors=True)
+    orc = oracle_mod.OracleSolver(scene)
+    pci = scene.params.solver == abi.LSP_SOLVER_PCISPH
+    for s in range(steps):
+        it = ref.step(scene.dt)
+        st = orc.step(scene.dt)
+        if pci:
+            assert it == st.iterations, f"step {s}"
+        ro, ri = ref.neighbors()
+        oo, oi = orc.neighbors()
+        assert np.array_equal(ro, oo) and np.array_equal(ri, oi), f"step {s}: neighbour lists"
+        for f in FIELDS + (PCI_FIELDS if pci else []):
+            assert same_bits(ref.get(f), orc.get(f)), f"step {s} field {f}"
+    ref.close()
+    orc.close()
+
+
+def test_tables_and_mass_match_reference(oracle_mod, need_ref):
+    for r, factor, rho0 in [(0.017, 2.688, 998.29), (0.0125, 3.2, 1000.0), (0.00459375, 3.2, 1000.0)]:
+        p = abi.default_params(particle_radius=r, kernel_radius_factor=factor, rest_density=rho0)
+        sc = scenes.Scene("t", p, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), [], 0.001, 0)
+        ref = oracle_mod.RefSolver(sc)
+        orc = oracle_mod.OracleSolver(sc)
+        assert same_bits(ref.tables(), orc.tables())
+        assert same_bits(ref.mass(), orc.mass())
+        assert same_bits(ref.kernel_radius(), orc.kernel_radius())
+
+
+def test_fp64_oracle_bounds_fp32_error(oracle_mod):
+    """States the FP32 error against the FP64 restatement after one step from the same input:
+    density and pressure within 1e-5 relative to rho0 (pressure: to delta * rho0 scale)."""
+    sc = scenes.small_box_scene(n_side=(10, 12, 10))
+    o32 = oracle_mod.OracleSolver(sc)
+    o64 = oracle_mod.OracleSolver(sc, fp64=True)
+    o32.step(sc.dt)
+    o64.step(sc.dt)
+    rho0 = sc.params.rest_density
+    d = np.abs(o32.get(abi.FIELD_DENSITY).astype(np.float64) - o64.get(abi.FIELD_DENSITY, fp64=True))
+    assert d.max() / rho0 < 1e-5
+    x = np.abs(o32.get(abi.FIELD_POSITION).astype(np.float64) - o64.get(abi.FIELD_POSITION, fp64=True))
+    assert x.max() < 1e-6
+
+
+def test_min_iteration_floor(oracle_mod):
+    sc = scenes.small_box_scene(pci_min_iterations=3, pci_max_iterations=50)
+    orc = oracle_mod.OracleSolver(sc)
+    for _ in range(3):
+        st = orc.step(sc.dt)
+        assert st.iterations >= 3
+        assert st.converged == 1
+
+
+def test_grid_spec_properties(oracle_mod):
+    sc = scenes.small_box_scene(n_side=(12, 9, 11))
+    h = 0.04
+    origin = np.array([0, 0, 0], np.int32)
+    dims = np.array([26, 26, 26], np.int32)
+    keys, ids, start, esc = oracle_mod.grid_build(sc.positions, h, origin, dims)
+    assert esc == 0
+    assert np.all(np.diff(keys.astype(np.int64)) >= 0)
+    same = np.diff(keys.astype(np.int64)) == 0
+    assert np.all(np.diff(ids)[same] > 0), "ids ascend inside a cell"
+    assert np.array_equal(start[:-1], np.searchsorted(keys, np.arange(start.size - 1)))
+    assert start[-1] == sc.n
+    c = (sc.positions / np.float32(h)).astype(np.int32)
+    k = (c[:, 0] * dims[1] + c[:, 1]) * dims[2] + c[:, 2]
+    assert np.array_equal(np.sort(k), keys)
+    # A smaller box clamps particles into edge cells and counts them.
+    keys2, ids2, start2, esc2 = oracle_mod.grid_build(sc.positions, h, origin, np.array([3, 3, 3], np.int32))
+    assert esc2 > 0 and start2[-1] == sc.n
+
+
+def test_scene_sizes_and_determinism():
+    assert scenes.dam_break_sph().n == 12000
+    assert scenes.dam_break_pcisph(counts=(64, 102, 64)).n == 417792
+    wb = scenes.wave_breaker()
+    assert wb.n == 108 * 68 * 136 == 998784
+    a = scenes.small_box_scene(seed=3).positions
+    b = scenes.small_box_scene(seed=3).positions
+    assert np.array_equal(a, b)
+    batch = scenes.batched_dam_breaks()
+    assert len(batch) == 64
+    ns = [s.n for s in batch]
+    assert min(ns) >= 1000 and max(ns) <= 70000
