@@ -51,6 +51,10 @@ extern "C" {
 #define LSP_WARM_ZERO      0   /* reference: p = 0, F_p = 0 (PCISPHSolver.cpp:58-62) */
 #define LSP_WARM_MLP       1   /* learned per-particle MLP guess, rejected if it raises the error */
 
+/* ---- PCISPH loop execution (results are identical) ---- */
+#define LSP_LOOP_PERSISTENT 0   /* one cooperative kernel, convergence decided on the device */
+#define LSP_LOOP_HOST       1   /* one launch per phase, convergence read back every iteration */
+
 /*
  * Solver parameters. Field meaning and defaults follow SPHSolver::SPHSolver
  * (SPHSolver.cpp:11-23) and PCISPHSolver::PCISPHSolver (PCISPHSolver.cpp:6-7);
@@ -76,7 +80,8 @@ typedef struct lsp_params {
     int32_t warm_start;                /* LSP_WARM_*; default LSP_WARM_ZERO */
     int32_t strict_convergence;        /* 1: lsp_step returns LSP_ERR_NOT_CONVERGED at max iterations */
     int32_t keep_initial_velocity;     /* 1: skip the reference's first-step velocity wipe in PCISPH (Delta 5) */
-    int32_t reserved[7];
+    int32_t loop_mode;                 /* LSP_LOOP_*: how the PCISPH loop runs; default LSP_LOOP_PERSISTENT */
+    int32_t reserved[6];
 } lsp_params;
 
 /* Per-step statistics, filled by lsp_step when non-NULL. */
@@ -169,6 +174,33 @@ int lsp_read_neighbors(lsp_solver* s, int64_t* offsets, int32_t* index, int64_t 
  * cell key and caller id per sorted slot, and the dense cell table (cells+1 entries). */
 int lsp_grid_info(lsp_solver* s, int32_t dims[3], int32_t origin[3], int64_t* cells);
 int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one);
+
+/* ---- measurement ---- */
+/* CUDA events on the solver's stream: mark records event `slot` (0..15); elapsed waits for
+ * slot_b and returns the device time between the two marks in milliseconds. */
+int lsp_timer_mark(lsp_solver* s, int slot);
+int lsp_timer_elapsed(lsp_solver* s, int slot_a, int slot_b, float* ms);
+/* Per-kernel-class device time: with profiling on, every launch is bracketed by events on
+ * the solver's stream. read: ms[k] and launches[k] for k < LSP_PROF_COUNT. */
+#define LSP_PROF_GRID_SORT     0   /* cell keys, histogram, scan, scatter, rank + gather */
+#define LSP_PROF_NEIGHBORS     1
+#define LSP_PROF_DENSITY       2
+#define LSP_PROF_NONPRESSURE   3
+#define LSP_PROF_SPH_PRESSURE  4
+#define LSP_PROF_PCI_PREDICT   5
+#define LSP_PROF_PCI_DENSITY   6
+#define LSP_PROF_PCI_FORCE     7
+#define LSP_PROF_INTEGRATE     8
+#define LSP_PROF_PCI_LOOP      9   /* the persistent predict-correct kernel */
+#define LSP_PROF_WARM_START    10
+#define LSP_PROF_COUNT         11
+int lsp_profile(lsp_solver* s, int enable);
+int lsp_profile_read(lsp_solver* s, double* ms, int64_t* launches, int capacity);
+/* Kernels this solver has launched since creation. */
+int lsp_launch_count(const lsp_solver* s, int64_t* launches);
+/* Page-locked host memory for asynchronous copies (cudaMallocHost / cudaFreeHost). */
+int lsp_host_alloc(size_t bytes, void** out);
+int lsp_host_free(void* p);
 
 #ifdef __cplusplus
 }

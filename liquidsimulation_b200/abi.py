@@ -28,6 +28,8 @@ LSP_OBSTACLE = 0
 LSP_BOUNDARY = 1
 LSP_WARM_ZERO = 0
 LSP_WARM_MLP = 1
+LSP_LOOP_PERSISTENT = 0
+LSP_LOOP_HOST = 1
 
 FIELD_POSITION = 0
 FIELD_VELOCITY = 1
@@ -46,6 +48,9 @@ FIELD_SPEED_SQUARED = 13
 
 VECTOR_FIELDS = {FIELD_POSITION, FIELD_VELOCITY, FIELD_HALF_VELOCITY, FIELD_PRED_POSITION,
                  FIELD_PRED_HALF_VELOCITY, FIELD_PRED_PRESSURE_FORCE, FIELD_OLD_HALF_VELOCITY}
+
+PROF_NAMES = ["grid_sort", "neighbors", "density", "nonpressure", "sph_pressure", "pci_predict",
+              "pci_density", "pci_force", "integrate_collide", "pci_loop", "warm_start"]
 
 TABLE_SIZE = 1001  # SPHKernel m_subdivision = 1000 -> 1001 entries (SPHKernel.cpp:4-7, :124)
 
@@ -71,7 +76,8 @@ class LspParams(ctypes.Structure):
         ("warm_start", c_int32),
         ("strict_convergence", c_int32),
         ("keep_initial_velocity", c_int32),
-        ("reserved", c_int32 * 7),
+        ("loop_mode", c_int32),
+        ("reserved", c_int32 * 6),
     ]
 
 
@@ -109,6 +115,7 @@ def default_params(**overrides) -> LspParams:
     p.warm_start = LSP_WARM_ZERO
     p.strict_convergence = 0
     p.keep_initial_velocity = 0
+    p.loop_mode = LSP_LOOP_PERSISTENT
     for k, v in overrides.items():
         if k == "gravity":
             p.gravity[:] = tuple(v)
@@ -194,6 +201,13 @@ def _declare(lib):
         "lsp_read_neighbors": (c_int, [S, i64p, i32p, c_int64, c_int64]),
         "lsp_grid_info": (c_int, [S, i32p, i32p, i64p]),
         "lsp_read_grid": (c_int, [S, u32p, i32p, c_int64, u32p, c_int64]),
+        "lsp_timer_mark": (c_int, [S, c_int]),
+        "lsp_timer_elapsed": (c_int, [S, c_int, c_int, fp]),
+        "lsp_profile": (c_int, [S, c_int]),
+        "lsp_profile_read": (c_int, [S, POINTER(c_double), i64p, c_int]),
+        "lsp_launch_count": (c_int, [S, i64p]),
+        "lsp_host_alloc": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
+        "lsp_host_free": (c_int, [c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -270,4 +270,40 @@ int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32
     return guard([&] { E(s).read_grid(keys, ids, n, cell_start, cells_plus_one); });
 }
 
+int lsp_timer_mark(lsp_solver* s, int slot)
+{
+    return guard([&] { E(s).timer_mark(slot); });
+}
+int lsp_timer_elapsed(lsp_solver* s, int slot_a, int slot_b, float* ms)
+{
+    return guard([&] { need(ms, "ms"); *ms = E(s).timer_elapsed(slot_a, slot_b); });
+}
+int lsp_profile(lsp_solver* s, int enable)
+{
+    return guard([&] { E(s).profile(enable != 0); });
+}
+int lsp_profile_read(lsp_solver* s, double* ms, int64_t* launches, int capacity)
+{
+    return guard([&] { E(s).profile_read(ms, launches, capacity); });
+}
+int lsp_launch_count(const lsp_solver* s, int64_t* launches)
+{
+    return guard([&] { need(launches, "launches"); *launches = E(s).launch_count(); });
+}
+int lsp_host_alloc(size_t bytes, void** out)
+{
+    return guard([&] {
+        need(out, "out");
+        *out = nullptr;
+        cudaError_t e = cudaMallocHost(out, bytes);
+        if (e != cudaSuccess) throw lsp::Error(LSP_ERR_CUDA, std::string("cudaMallocHost: ") + cudaGetErrorString(e));
+    });
+}
+int lsp_host_free(void* p)
+{
+    return guard([&] {
+        if (p) cudaFreeHost(p);
+    });
+}
+
 }  // extern "C"

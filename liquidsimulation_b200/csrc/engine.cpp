@@ -124,6 +124,7 @@ static void validate(const lsp_params& p)
     if (p.pci_max_iterations < 0 || p.pci_max_iterations > kMaxIterationsCap) bad("pci_max_iterations out of range [0, 1024]");
     if (p.pci_min_iterations < 0) bad("pci_min_iterations must be >= 0");
     if (p.warm_start != LSP_WARM_ZERO && p.warm_start != LSP_WARM_MLP) bad("unknown warm_start");
+    if (p.loop_mode != LSP_LOOP_PERSISTENT && p.loop_mode != LSP_LOOP_HOST) bad("unknown loop_mode");
 }
 
 Engine::Engine(const lsp_params& p, int device)
@@ -144,6 +145,8 @@ Engine::Engine(const lsp_params& p, int device)
     std::memset(hstatus_, 0, sizeof(DevStatus));
     status_.alloc(1);
     bounds_.alloc(6);
+    loop_sync_.alloc(4);
+    maxerr_.alloc(kMaxIterationsCap);
     prm_ = p;
     derive();
 }
@@ -153,6 +156,9 @@ Engine::~Engine()
     cudaSetDevice(dev_);
     if (stream_) cudaStreamSynchronize(stream_);
     if (hstatus_) cudaFreeHost(hstatus_);
+    for (cudaEvent_t e : evpool_) cudaEventDestroy(e);
+    for (cudaEvent_t e : marks_)
+        if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -196,15 +202,17 @@ void Engine::ensure_capacity(int64_t n)
     std::swap(slot_of_id_.p, nsoi.p), std::swap(slot_of_id_.n, nsoi.n);
     for (int k = 0; k < 4; k++) np[k].release();
     pos_[1 - cur_].alloc(cap); vel_[1 - cur_].alloc(cap); half_[1 - cur_].alloc(cap); old_[1 - cur_].alloc(cap);
-    force_.alloc(cap); ppos_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
-    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap); sfac_.alloc(cap);
+    force_.alloc(cap); ppos_.alloc(cap); ppos_alt_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
+    ppos_final_ = ppos_.p;
+    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap);
     key_.alloc(cap); slot_.alloc(cap); sorted_key_.alloc(cap); tmp_.alloc(cap); nbr_count_.alloc(cap);
     stage_.alloc(cap * 12);
     CK(cudaMemsetAsync(force_.p, 0, cap * sizeof(float4), stream_));
     CK(cudaMemsetAsync(ppos_.p, 0, cap * sizeof(float4), stream_));
+    CK(cudaMemsetAsync(ppos_alt_.p, 0, cap * sizeof(float4), stream_));
     CK(cudaMemsetAsync(phalf_.p, 0, cap * sizeof(float4), stream_));
     CK(cudaMemsetAsync(pforce_.p, 0, cap * sizeof(float4), stream_));
-    for (DevArray<float>* a : {&rho_, &pres_, &prho_, &err_, &sfac_})
+    for (DevArray<float>* a : {&rho_, &pres_, &prho_, &err_})
         CK(cudaMemsetAsync(a->p, 0, cap * sizeof(float), stream_));
     CK(cudaMemsetAsync(nbr_count_.p, 0, cap * sizeof(int32_t), stream_));
     cap_ = cap;
@@ -408,22 +416,112 @@ StepBuffers Engine::buffers()
     StepBuffers b{};
     b.pos = pos_[cur_].p; b.vel = vel_[cur_].p; b.half = half_[cur_].p; b.old = old_[cur_].p;
     b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
-    b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p; b.sfac = sfac_.p;
+    b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
     b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p;
     return b;
 }
 
-void Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st)
+template <typename F>
+void Engine::timed(int cls, F&& launch)
 {
+    if (!profile_) {
+        launches_ += launch();
+        return;
+    }
+    while (evpool_.size() < evnext_ + 2) {
+        cudaEvent_t e;
+        CK(cudaEventCreate(&e));
+        evpool_.push_back(e);
+    }
+    size_t first = evnext_;
+    evnext_ += 2;
+    CK(cudaEventRecord(evpool_[first], stream_));
+    int n = launch();
+    CK(cudaEventRecord(evpool_[first + 1], stream_));
+    launches_ += n;
+    prof_n_[cls] += n;
+    pending_.push_back({cls, first});
+}
+
+// Called after a stream synchronisation: folds the bracketed intervals into the totals.
+void Engine::collect_profile()
+{
+    for (auto& pr : pending_) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, evpool_[pr.second], evpool_[pr.second + 1]));
+        prof_ms_[pr.first] += ms;
+    }
+    pending_.clear();
+    evnext_ = 0;
+}
+
+void Engine::profile(bool on)
+{
+    activate();
+    CK(cudaStreamSynchronize(stream_));
+    collect_profile();
+    profile_ = on;
+    for (int k = 0; k < LSP_PROF_COUNT; k++) { prof_ms_[k] = 0.0; prof_n_[k] = 0; }
+}
+
+void Engine::profile_read(double* ms, int64_t* launches, int capacity)
+{
+    activate();
+    CK(cudaStreamSynchronize(stream_));
+    collect_profile();
+    for (int k = 0; k < LSP_PROF_COUNT && k < capacity; k++) {
+        if (ms) ms[k] = prof_ms_[k];
+        if (launches) launches[k] = prof_n_[k];
+    }
+}
+
+void Engine::timer_mark(int slot)
+{
+    if (slot < 0 || slot >= 16) throw Error(LSP_ERR_INVALID, "timer slot must be in [0, 16)");
+    activate();
+    if (!marks_[slot]) CK(cudaEventCreate(&marks_[slot]));
+    CK(cudaEventRecord(marks_[slot], stream_));
+}
+
+float Engine::timer_elapsed(int a, int b)
+{
+    if (a < 0 || a >= 16 || b < 0 || b >= 16 || !marks_[a] || !marks_[b])
+        throw Error(LSP_ERR_INVALID, "timer slots not marked");
+    activate();
+    CK(cudaEventSynchronize(marks_[b]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, marks_[a], marks_[b]));
+    return ms;
+}
+
+bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st)
+{
+    ppos_final_ = ppos_.p;
+    if (P.max_it <= 0) {
+        CK(cudaMemsetAsync(pforce_.p, 0, n_ * sizeof(float4), stream_));
+        if (st) { st->iterations = 0; st->converged = 0; st->max_density_error_ratio = 0.0; }
+        return false;
+    }
+    if (prm_.loop_mode == LSP_LOOP_PERSISTENT) {
+        CK(cudaMemsetAsync(loop_sync_.p, 0, 4 * sizeof(uint32_t), stream_));
+        CK(cudaMemsetAsync(maxerr_.p, 0, (size_t)P.max_it * sizeof(uint32_t), stream_));
+        bool ok = false;
+        int grid = 0;
+        timed(LSP_PROF_PCI_LOOP, [&] {
+            ok = launch_pci_loop(P, b, ppos_alt_.p, loop_sync_.p, maxerr_.p, stream_, &grid);
+            return ok ? 1 : 0;
+        });
+        if (ok) return true;
+        cudaGetLastError();   // a refused cooperative launch leaves a sticky-free error; fall back
+    }
     int it = 0;
     bool conv = false;
     float maxErr = 0.f, ratio = 0.f;
-    if (P.max_it <= 0) CK(cudaMemsetAsync(pforce_.p, 0, n_ * sizeof(float4), stream_));
     for (int k = 0; k < P.max_it; k++) {
-        launch_pci_predict(P, b, k, stream_);
-        launch_pci_density(P, b, k, stream_);
-        launch_pci_force(P, b, stream_);
+        timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, k, stream_); return 1; });
+        timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, k, stream_); return 1; });
+        timed(LSP_PROF_PCI_FORCE, [&] { launch_pci_force(P, b, stream_); return 1; });
         it = k + 1;
         CK(cudaMemcpyAsync(&hstatus_->max_err_bits, &status_.p->max_err_bits, sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, stream_));
@@ -438,6 +536,7 @@ void Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         st->converged = conv ? 1 : 0;
         st->max_density_error_ratio = (double)maxErr / (double)prm_.rest_density;
     }
+    return false;
 }
 
 static int initial_neighbor_capacity(const lsp_params& p)
@@ -469,7 +568,9 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
     if (!dcols_.p) upload_colliders();
     if (nbr_cap_ == 0 || nbr_stride_ < cap_) ensure_neighbors(nbr_cap_ ? nbr_cap_ : initial_neighbor_capacity(prm_));
     lsp_step_stats local{};
+    bool device_loop = false;
     for (int attempt = 0;; attempt++) {
+        device_loop = false;
         DevParams P = device_params(dt);
         CK(cudaMemsetAsync(status_.p, 0, sizeof(DevStatus), stream_));
         GridBuildArgs g{};
@@ -480,23 +581,25 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
         g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
         g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
-        launch_grid_build(g, stream_);
+        timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_sort(g, stream_); });
+        timed(LSP_PROF_NEIGHBORS, [&] { return launch_neighbors(g, stream_); });
         cur_ = 1 - cur_;
         StepBuffers b = buffers();
-        launch_density(P, b, stream_);
-        launch_nonpressure(P, b, stream_);
+        timed(LSP_PROF_DENSITY, [&] { launch_density(P, b, stream_); return 1; });
+        timed(LSP_PROF_NONPRESSURE, [&] { launch_nonpressure(P, b, stream_); return 1; });
         if (prm_.solver == LSP_SOLVER_SPH) {
-            launch_sph_pressure(P, b, stream_);
-            launch_integrate_collide(P, b, false, stream_);
+            timed(LSP_PROF_SPH_PRESSURE, [&] { launch_sph_pressure(P, b, stream_); return 1; });
+            timed(LSP_PROF_INTEGRATE, [&] { launch_integrate_collide(P, b, false, stream_); return 1; });
             local.iterations = 0;
             local.converged = 1;
         } else {
-            pcisph_loop(P, b, &local);
-            launch_integrate_collide(P, b, true, stream_);
+            device_loop = pcisph_loop(P, b, &local);
+            timed(LSP_PROF_INTEGRATE, [&] { launch_integrate_collide(P, b, true, stream_); return 1; });
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hstatus_, status_.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
+        if (profile_) collect_profile();
         if ((hstatus_->error_flags & kErrNeighborOverflow) && attempt < 3) {
             cur_ = 1 - cur_;   // the gather left the pre-step state untouched: redo the step
             ensure_neighbors((int)hstatus_->max_neighbors + (int)hstatus_->max_neighbors / 4 + 8);
@@ -505,10 +608,20 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         break;
     }
     stepped_ = true;
+    if (device_loop) {
+        float me;
+        std::memcpy(&me, &hstatus_->max_err_bits, 4);
+        local.iterations = hstatus_->iterations;
+        local.converged = hstatus_->converged;
+        local.max_density_error_ratio = (double)me / (double)prm_.rest_density;
+        ppos_final_ = ((local.iterations - 1) & 1) ? ppos_alt_.p : ppos_.p;
+    }
     local.max_neighbors = (int32_t)hstatus_->max_neighbors;
     local.escaped = (int32_t)hstatus_->escaped;
     if (st) *st = local;
     if (hstatus_->escaped && domain_from_particles_) grid_valid_ = false;
+    if (hstatus_->error_flags & kErrTimeout)
+        throw Error(LSP_ERR_TIMEOUT, "a grid barrier of the persistent PCISPH loop gave up");
     if (hstatus_->error_flags & kErrNeighborOverflow)
         throw Error(LSP_ERR_CAPACITY, "neighbour list overflow persisted after resizing");
     if (hstatus_->error_flags & kErrScan)
@@ -550,7 +663,7 @@ void Engine::read_field(int field, float* out, int64_t n)
     case LSP_FIELD_VELOCITY: src = vel_[cur_].p; comps = 3; break;
     case LSP_FIELD_HALF_VELOCITY: src = half_[cur_].p; comps = 3; break;
     case LSP_FIELD_OLD_HALF_VELOCITY: src = old_[cur_].p; comps = 3; break;
-    case LSP_FIELD_PRED_POSITION: src = ppos_.p; comps = 3; break;
+    case LSP_FIELD_PRED_POSITION: src = ppos_final_ ? ppos_final_ : ppos_.p; comps = 3; break;
     case LSP_FIELD_PRED_HALF_VELOCITY: src = phalf_.p; comps = 3; break;
     case LSP_FIELD_PRED_PRESSURE_FORCE: src = pforce_.p; comps = 3; break;
     case LSP_FIELD_DENSITY: src = rho_.p; break;

@@ -70,6 +70,13 @@ public:
     void grid_info(int32_t dims[3], int32_t origin[3], int64_t* cells) const;
     void read_grid(uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one);
 
+    // Measurement (lsp_timer_*, lsp_profile*, lsp_launch_count).
+    void timer_mark(int slot);
+    float timer_elapsed(int a, int b);
+    void profile(bool on);
+    void profile_read(double* ms, int64_t* launches, int capacity);
+    int64_t launch_count() const { return launches_; }
+
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
     // Device order view for in-library callers (kernel timing, the MLP).
@@ -84,7 +91,8 @@ private:
     void ensure_neighbors(int cap);
     void upload_colliders();
     void run_step(float dt, lsp_step_stats* st, bool final_sync);
-    void pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st);
+    // Returns true when the persistent device loop ran (its stats arrive with the status).
+    bool pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st);
     void stage(size_t floats);
 
     lsp_params prm_{};
@@ -95,8 +103,10 @@ private:
     int64_t n_ = 0, cap_ = 0;
     int cur_ = 0;
     DevArray<float4> pos_[2], vel_[2], half_[2], old_[2];
-    DevArray<float4> force_, ppos_, phalf_, pforce_;
-    DevArray<float> rho_, pres_, prho_, err_, sfac_;
+    DevArray<float4> force_, ppos_, ppos_alt_, phalf_, pforce_;
+    const float4* ppos_final_ = nullptr;   // buffer holding the last iteration's x*
+    DevArray<uint32_t> loop_sync_, maxerr_;
+    DevArray<float> rho_, pres_, prho_, err_;
     DevArray<uint32_t> key_, slot_, sorted_key_;
     DevArray<int2> tmp_;
     DevArray<int32_t> slot_of_id_, nbr_, nbr_count_;
@@ -118,6 +128,19 @@ private:
     DevArray<DevStatus> status_;
     DevStatus* hstatus_ = nullptr;   // pinned
     DevArray<float> stage_;
+
+    // Launch bracketing for the per-class profile.
+    template <typename F>
+    void timed(int cls, F&& launch);
+    void collect_profile();
+    cudaEvent_t marks_[16] = {};
+    bool profile_ = false;
+    std::vector<cudaEvent_t> evpool_;
+    size_t evnext_ = 0;
+    std::vector<std::pair<int, size_t>> pending_;   // (class, first event index)
+    double prof_ms_[LSP_PROF_COUNT] = {};
+    int64_t prof_n_[LSP_PROF_COUNT] = {};
+    int64_t launches_ = 0;
     DevArray<int32_t> bounds_;
     bool stepped_ = false;
 };

@@ -249,7 +249,9 @@ __global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const u
                 }
             }
         }
-        count[i] = c;
+        // The stored count never exceeds the list capacity, so later passes stay inside the
+        // list even in an overflowed step; the true count only feeds the maximum below.
+        count[i] = min(c, cap);
     }
     // Overflow flag and the step's maximum count: one atomic per warp.
     uint32_t m = (uint32_t)c;
@@ -265,24 +267,37 @@ __global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const u
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-void launch_grid_build(const GridBuildArgs& a, cudaStream_t s)
+int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;
     const DevParams& P = a.P;
-    if (P.n > 0)
+    int launches = 0;
+    if (P.n > 0) {
         k_keys_hist<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.hist, a.status);
+        launches++;
+    }
     const int64_t n = (int64_t)P.cells + 1;
     const int tiles = (int)((n + kScanTile - 1) / kScanTile);
     k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
     k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
     k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
+    launches += 3;
     if (P.n > 0) {
         k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
         k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
                                                        a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
                                                        a.old_out, a.slot_of_id, a.sorted_key, a.status);
-        k_neighbors<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
+        launches += 2;
     }
+    return launches;
+}
+
+int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)
+{
+    const int T = 256;
+    if (a.P.n <= 0) return 0;
+    k_neighbors<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
+    return 1;
 }
 
 }  // namespace lsp

@@ -46,7 +46,6 @@ struct StepBuffers {
     float4* pforce;
     float* prho;
     float* err;
-    float* sfac;      // p / rho*^2 of each particle, the pressure-force factor
     // neighbours
     const int32_t* nbr;
     const int32_t* nbr_count;
@@ -56,7 +55,9 @@ struct StepBuffers {
     DevStatus* status;
 };
 
-void launch_grid_build(const GridBuildArgs& a, cudaStream_t s);
+// Both return the number of kernels launched.
+int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
+int launch_neighbors(const GridBuildArgs& a, cudaStream_t s);
 
 void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);
@@ -68,7 +69,9 @@ void launch_pci_density(const DevParams& P, const StepBuffers& b, int iteration,
 void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // Whole predict-correct loop in one cooperative persistent launch; returns false when the
 // device cannot co-schedule the grid (the caller then uses the per-phase launches).
-bool launch_pci_loop(const DevParams& P, const StepBuffers& b, cudaStream_t s, int* grid_used);
+// ppos_alt: second predicted-position buffer; sync: 16 zeroed bytes; maxerr: max_it zeroed words.
+bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
+                     cudaStream_t s, int* grid_used);
 
 // Gathers a per-particle field from device order into caller order.
 // comps: 1 (float) or 3 (xyz of a float4); src is float* or float4* accordingly.

@@ -6,7 +6,9 @@ The reference ships no scene files or datasets; its demo builds scenes in code
 for them with seeded lattices: lattice point (i, j, k) sits at
 ``lo + (i + 0.5) * s`` and is jittered uniformly by +-1 % of the spacing per axis,
 drawn from ``numpy.random.Generator(PCG64(seed))`` in x, y, z order per particle.
-Particles are emitted x-fastest (i inner, then j, then k).
+Particles are emitted x-fastest (i inner, then j, then k). Blocks that rest against
+the walls start one particle radius plus the jitter amplitude from each wall
+(``wall_lattice``), so their first layer is not moved by the first collision pass.
 
 Particle radius is ``s / 1.6`` (the emitter's spacing is 1.6 radii,
 SPHParticleEmitter.cpp) and the smoothing length ``h = 2 s``, i.e. a kernel-radius
@@ -48,15 +50,31 @@ class Scene:
         return int(self.positions.shape[0])
 
 
-def lattice(lo, counts, s, seed, jitter=0.01, rng=None):
-    """Jittered lattice: counts=(nx, ny, nz) points at lo + (idx + 0.5) * s, x fastest."""
+def lattice(lo, counts, s, seed, jitter=0.01, rng=None, first=None):
+    """Jittered lattice: counts=(nx, ny, nz) points at lo + (idx + 0.5) * s, x fastest, or at
+    first + idx * s when ``first`` (the first point per axis) is given."""
     nx, ny, nz = (int(c) for c in counts)
     rng = rng if rng is not None else np.random.Generator(np.random.PCG64(seed))
     k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
     base = np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1).astype(np.float64)
-    pts = np.asarray(lo, np.float64)[None, :] + (base + 0.5) * s
+    if first is not None:
+        pts = np.asarray(first, np.float64)[None, :] + base * s
+    else:
+        pts = np.asarray(lo, np.float64)[None, :] + (base + 0.5) * s
     pts += rng.uniform(-jitter * s, jitter * s, size=pts.shape)
     return pts.astype(np.float32)
+
+
+def wall_lattice(lo, counts, s, seed, rng=None):
+    """A block resting in a corner of the walls at ``lo``: its first layer sits one particle
+    radius (s / 1.6) plus the jitter amplitude from each wall, so the boundary collision
+    (which keeps particles r inside, StaticCollisionBox.cpp:77-114) does not move it. A
+    block starting at lo + s/2 would have its first layer pinned 1/8 spacing inward by the
+    first collision pass, which compresses the corner by ~20 % and makes the reference's
+    PCISPH loop run to its iteration cap."""
+    off = s / 1.6 + 0.01 * s
+    first = tuple(float(l) + off for l in lo)
+    return lattice(lo, counts, s, seed, rng=rng, first=first)
 
 
 def _params(s, solver, **kw):
@@ -83,7 +101,7 @@ def dam_break_sph(seed: int = 1, scale: float = 1.0) -> Scene:
     mass 0.008, h = 0.04, k = 3, mu = 0.1, dt = 0.002. ``scale`` < 1 shrinks the block."""
     s = 0.02
     counts = [max(2, int(round(c * scale))) for c in (20, 30, 20)]
-    pos = lattice((0.0, 0.0, 0.0), counts, s, seed)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed)
     p = _params(s, abi.LSP_SOLVER_SPH, mass_override=0.008)
     box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
     return Scene("dam_break_sph_12k", p, pos, np.zeros_like(pos), [box], 0.002, 1000,
@@ -93,7 +111,7 @@ def dam_break_sph(seed: int = 1, scale: float = 1.0) -> Scene:
 def dam_break_pcisph(seed: int = 2, counts=(64, 102, 64), s: float = 0.00625) -> Scene:
     """PCISPH dam break: unit box walls, 64x102x64 block at s = 0.00625 (417,792 particles),
     h = 2 s, eta = 1 %, min 3 / max 50 iterations, zero initial pressure, dt = 0.001."""
-    pos = lattice((0.0, 0.0, 0.0), counts, s, seed)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed)
     p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
     box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
     n = int(np.prod(counts))
@@ -108,7 +126,7 @@ def wave_breaker(seed: int = 3, s: float = 0.00735, block=(0.8, 0.5, 1.0)) -> Sc
     min 3 / max 50, dt = 0.0008."""
     rng = np.random.Generator(np.random.PCG64(seed))
     counts = [int(math.floor(b / s + 1e-9)) for b in block]
-    pos = lattice((0.0, 0.0, 0.0), counts, s, seed, rng=rng)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed, rng=rng)
     p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
     cols = [Collider("box", (1.0, 0.5, 0.5), (1.0, 0.5, 0.5), True)]
     for _ in range(2):
@@ -132,7 +150,7 @@ def batched_dam_breaks(seed: int = 4, scenes: int = 64, nmin: int = 2000, nmax: 
         edges = rng.uniform(0.2, 0.6, size=3)
         s = float((np.prod(edges) / n_target) ** (1.0 / 3.0))
         counts = [max(2, int(e / s)) for e in edges]
-        pos = lattice((0.0, 0.0, 0.0), counts, s, int(rng.integers(1 << 30)))
+        pos = wall_lattice((0.0, 0.0, 0.0), counts, s, int(rng.integers(1 << 30)))
         p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
         box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
         out.append(Scene(f"batch_{b}", p, pos, np.zeros_like(pos), [box], 0.001, 100,

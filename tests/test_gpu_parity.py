@@ -107,9 +107,22 @@ def test_dam_break_sph_12k_bit_exact(oracle_mod):
     gpu.close()
 
 
-def test_pcisph_min_max_iterations(oracle_mod):
-    sc = scenes.small_box_scene(n_side=(12, 14, 12), pci_min_iterations=3, pci_max_iterations=50)
+@pytest.mark.parametrize("loop_mode", [abi.LSP_LOOP_PERSISTENT, abi.LSP_LOOP_HOST])
+def test_pcisph_min_max_iterations(oracle_mod, loop_mode):
+    sc = scenes.small_box_scene(n_side=(12, 14, 12), pci_min_iterations=3, pci_max_iterations=50,
+                                loop_mode=loop_mode)
     gpu, orc = run_pair(oracle_mod, sc, 4, check_neighbors=False)
+    gpu.close()
+
+
+@pytest.mark.parametrize("loop_mode", [abi.LSP_LOOP_PERSISTENT, abi.LSP_LOOP_HOST])
+def test_pcisph_loop_modes_many_iterations(oracle_mod, loop_mode):
+    """A tight tolerance forces long loops (the persistent kernel crosses many grid barriers)."""
+    sc = scenes.small_box_scene(n_side=(16, 16, 16), pci_eta=1e-4, pci_min_iterations=1,
+                                pci_max_iterations=40, loop_mode=loop_mode)
+    gpu, orc = run_pair(oracle_mod, sc, 3, check_neighbors=False)
+    st = gpu.update(sc.dt)
+    assert st.iterations > 5
     gpu.close()
 
 
