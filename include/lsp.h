@@ -175,6 +175,30 @@ int lsp_read_neighbors(lsp_solver* s, int64_t* offsets, int32_t* index, int64_t 
 int lsp_grid_info(lsp_solver* s, int32_t dims[3], int32_t origin[3], int64_t* cells);
 int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one);
 
+/* ---- learned warm start (warm_start = LSP_WARM_MLP) ----
+ * A per-particle MLP (8 features -> 32 -> 32 -> 1, SiLU, BF16 tensor-core MMA with FP32
+ * accumulation) guesses each particle's PCISPH pressure; the loop then iterates to the
+ * same eta. If the guess raises the maximum density error of the first correction, the
+ * step restarts from zero pressure and ends bit-identical to the plain solver.
+ * No counterpart in the reference. Parameters: FP32 vector of LSP_MLP_PARAMS floats,
+ * W1[8][32], b1[32], W2[32][32], b2[32], W3[32], b3. */
+#define LSP_MLP_PARAMS 1377
+#define LSP_MLP_FEATURES 8
+int lsp_mlp_reset(lsp_solver* s, uint64_t seed);                   /* random init, Adam state cleared */
+int lsp_mlp_set_weights(lsp_solver* s, const float* w, int n);
+int lsp_mlp_get_weights(lsp_solver* s, float* w, int n);
+/* Records the 8 features of every particle at iteration 0 of each PCISPH step. */
+int lsp_mlp_record(lsp_solver* s, int enable);
+/* Adam steps on the last recorded step: features -> final pressure (normalised).
+ * Each iteration draws `batch` random particles. loss (may be NULL): mean 0.5 (y - t)^2. */
+int lsp_mlp_train(lsp_solver* s, int iterations, int batch, float learning_rate, uint64_t seed, float* loss);
+/* Network output for n feature rows (host arrays float[8n] -> float[n]). */
+int lsp_mlp_forward(lsp_solver* s, const float* features, int64_t n, float* out);
+/* Gradient of 1/(2n) sum (y - t)^2 at the current weights (host arrays); no update. */
+int lsp_mlp_gradient(lsp_solver* s, const float* features, const float* targets, int64_t n, float* grad, float* loss);
+/* Features of the last recorded step, caller order, float[8n]. */
+int lsp_read_features(lsp_solver* s, float* out, int64_t n);
+
 /* ---- measurement ---- */
 /* CUDA events on the solver's stream: mark records event `slot` (0..15); elapsed waits for
  * slot_b and returns the device time between the two marks in milliseconds. */

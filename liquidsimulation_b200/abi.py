@@ -52,6 +52,9 @@ VECTOR_FIELDS = {FIELD_POSITION, FIELD_VELOCITY, FIELD_HALF_VELOCITY, FIELD_PRED
 PROF_NAMES = ["grid_sort", "neighbors", "density", "nonpressure", "sph_pressure", "pci_predict",
               "pci_density", "pci_force", "integrate_collide", "pci_loop", "warm_start"]
 
+MLP_PARAMS = 1377
+MLP_FEATURES = 8
+
 TABLE_SIZE = 1001  # SPHKernel m_subdivision = 1000 -> 1001 entries (SPHKernel.cpp:4-7, :124)
 
 
@@ -208,6 +211,14 @@ def _declare(lib):
         "lsp_launch_count": (c_int, [S, i64p]),
         "lsp_host_alloc": (c_int, [ctypes.c_size_t, POINTER(c_void_p)]),
         "lsp_host_free": (c_int, [c_void_p]),
+        "lsp_mlp_reset": (c_int, [S, ctypes.c_uint64]),
+        "lsp_mlp_set_weights": (c_int, [S, fp, c_int]),
+        "lsp_mlp_get_weights": (c_int, [S, fp, c_int]),
+        "lsp_mlp_record": (c_int, [S, c_int]),
+        "lsp_mlp_train": (c_int, [S, c_int, c_int, c_float, ctypes.c_uint64, fp]),
+        "lsp_mlp_forward": (c_int, [S, fp, c_int64, fp]),
+        "lsp_mlp_gradient": (c_int, [S, fp, fp, c_int64, fp, fp]),
+        "lsp_read_features": (c_int, [S, fp, c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -146,8 +146,9 @@ int lsp_kernel_tables(const lsp_solver* s, float* out, int capacity)
     return guard([&] {
         need(out, "out");
         const auto& t = E(s).tables();
-        if (capacity < (int)t.size()) throw lsp::Error(LSP_ERR_INVALID, "capacity below 5*1001");
-        std::memcpy(out, t.data(), t.size() * sizeof(float));
+        const int n = 5 * lsp::kTableSize;
+        if (capacity < n) throw lsp::Error(LSP_ERR_INVALID, "capacity below 5*1001");
+        std::memcpy(out, t.data(), n * sizeof(float));
     });
 }
 
@@ -268,6 +269,45 @@ int lsp_grid_info(lsp_solver* s, int32_t dims[3], int32_t origin[3], int64_t* ce
 int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one)
 {
     return guard([&] { E(s).read_grid(keys, ids, n, cell_start, cells_plus_one); });
+}
+
+int lsp_mlp_reset(lsp_solver* s, uint64_t seed)
+{
+    return guard([&] { E(s).mlp_reset(seed); });
+}
+int lsp_mlp_set_weights(lsp_solver* s, const float* w, int n)
+{
+    return guard([&] { E(s).mlp_set(w, n); });
+}
+int lsp_mlp_get_weights(lsp_solver* s, float* w, int n)
+{
+    return guard([&] { E(s).mlp_get(w, n); });
+}
+int lsp_mlp_record(lsp_solver* s, int enable)
+{
+    return guard([&] { E(s).mlp_record(enable != 0); });
+}
+int lsp_mlp_train(lsp_solver* s, int iterations, int batch, float learning_rate, uint64_t seed, float* loss)
+{
+    return guard([&] {
+        float l = E(s).mlp_train(iterations, batch, learning_rate, seed);
+        if (loss) *loss = l;
+    });
+}
+int lsp_mlp_forward(lsp_solver* s, const float* features, int64_t n, float* out)
+{
+    return guard([&] { E(s).mlp_forward(features, n, out); });
+}
+int lsp_mlp_gradient(lsp_solver* s, const float* features, const float* targets, int64_t n, float* grad, float* loss)
+{
+    return guard([&] {
+        float l = E(s).mlp_gradient(features, targets, n, grad);
+        if (loss) *loss = l;
+    });
+}
+int lsp_read_features(lsp_solver* s, float* out, int64_t n)
+{
+    return guard([&] { E(s).read_features(out, n); });
 }
 
 int lsp_timer_mark(lsp_solver* s, int slot)

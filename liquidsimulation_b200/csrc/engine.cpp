@@ -1,9 +1,12 @@
 // Host engine: device memory, grid box, step sequencing. See engine.h.
 #include "engine.h"
+#include "mlp.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
+#include <random>
 
 namespace lsp {
 
@@ -33,7 +36,8 @@ void HostKernels::build(const lsp_params& p)
     float poly_d2 = (float)(-945.0 / (32.0 * pi * (double)r9));
     float spiky_d1 = (float)(-45.0 / (pi * (double)r6));
     float visc_d2 = (float)(45.0 / (pi * (double)r6));
-    tables.assign(5 * kTableSize, 0.f);
+    // Five lookup tables, then the kTableSize + 1 slot thresholds of the device lookup.
+    tables.assign(6 * kTableSize + 1, 0.f);
     for (int i = 0; i <= sub; i++) {
         float d = i * step;
         float t = r2 - d * d;
@@ -44,6 +48,24 @@ void HostKernels::build(const lsp_params& p)
         tables[3 * kTableSize + i] = spiky_d1 * s * s;
         tables[4 * kTableSize + i] = visc_d2 * (h - d);
     }
+    // thr[k] = smallest float d >= 0 with (int)(d / step) >= k, by bisection over the
+    // ordered bit patterns of non-negative floats; thr[1001] = +inf.
+    float* thr = tables.data() + 5 * kTableSize;
+    thr[0] = 0.f;
+    const float hi_d = 2.f * h;
+    uint32_t hi_bits;
+    std::memcpy(&hi_bits, &hi_d, 4);
+    for (int k = 1; k <= sub; k++) {
+        uint32_t lo = 0, hi = hi_bits;
+        while (lo < hi) {
+            uint32_t mid = lo + (hi - lo) / 2;
+            float d;
+            std::memcpy(&d, &mid, 4);
+            if ((int)(d / step) >= k) hi = mid; else lo = mid + 1;
+        }
+        std::memcpy(&thr[k], &lo, 4);
+    }
+    thr[kTableSize] = std::numeric_limits<float>::infinity();
     float stepSize = 1.6f * p.particle_radius;
     float sum = 0.f;
     for (int i = -3; i <= 3; i++)
@@ -149,6 +171,7 @@ Engine::Engine(const lsp_params& p, int device)
     maxerr_.alloc(kMaxIterationsCap);
     prm_ = p;
     derive();
+    mlp_reset(0);
 }
 
 Engine::~Engine()
@@ -201,6 +224,20 @@ void Engine::ensure_capacity(int64_t n)
     for (int k = 0; k < 4; k++) std::swap(cur[k]->p, np[k].p), std::swap(cur[k]->n, np[k].n);
     std::swap(slot_of_id_.p, nsoi.p), std::swap(slot_of_id_.n, nsoi.n);
     for (int k = 0; k < 4; k++) np[k].release();
+    if (phist_[cur_].p) {
+        DevArray<float4> nh;
+        nh.alloc(cap);
+        CK(cudaMemsetAsync(nh.p, 0, cap * sizeof(float4), stream_));
+        if (n_ > 0) CK(cudaMemcpyAsync(nh.p, phist_[cur_].p, n_ * sizeof(float4), cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        std::swap(phist_[cur_].p, nh.p);
+        std::swap(phist_[cur_].n, nh.n);
+        phist_[1 - cur_].alloc(cap);
+        feat_.alloc(cap * kMlpIn);
+        gradrho_.alloc(cap);
+        tgt_.alloc(cap);
+        features_valid_ = false;
+    }
     pos_[1 - cur_].alloc(cap); vel_[1 - cur_].alloc(cap); half_[1 - cur_].alloc(cap); old_[1 - cur_].alloc(cap);
     force_.alloc(cap); ppos_.alloc(cap); ppos_alt_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
     ppos_final_ = ppos_.p;
@@ -251,6 +288,7 @@ void Engine::add_particles(const float* xyz, const float* vel, int64_t m)
     CK(cudaMemcpyAsync(half_[cur_].p + n_, z.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(old_[cur_].p + n_, z.data(), m * sizeof(float4), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(slot_of_id_.p + n_, soi.data(), m * sizeof(int32_t), cudaMemcpyHostToDevice, stream_));
+    if (phist_[cur_].p) CK(cudaMemsetAsync(phist_[cur_].p + n_, 0, m * sizeof(float4), stream_));
     CK(cudaStreamSynchronize(stream_));
     n_ += m;
     if (domain_from_particles_) grid_valid_ = false;
@@ -385,6 +423,7 @@ DevParams Engine::device_params(float dt) const
     P.h = hk_.h;
     P.h2 = hk_.h * hk_.h;
     P.step = hk_.step;
+    P.inv_step = 1.f / hk_.step;
     P.radius = prm_.particle_radius;
     P.mass = hk_.mass;
     P.rho0 = prm_.rest_density;
@@ -419,6 +458,8 @@ StepBuffers Engine::buffers()
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
     b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p;
+    b.hist = phist_[cur_].p;
+    b.gradrho = features_on() ? gradrho_.p : nullptr;
     return b;
 }
 
@@ -495,6 +536,11 @@ float Engine::timer_elapsed(int a, int b)
     return ms;
 }
 
+bool Engine::features_on() const
+{
+    return prm_.solver == LSP_SOLVER_PCISPH && (record_ || prm_.warm_start == LSP_WARM_MLP);
+}
+
 bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st)
 {
     ppos_final_ = ppos_.p;
@@ -503,38 +549,85 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         if (st) { st->iterations = 0; st->converged = 0; st->max_density_error_ratio = 0.0; }
         return false;
     }
+    const bool feats = features_on();
+    const bool warm = prm_.warm_start == LSP_WARM_MLP;
+    WarmArgs w{};
+    if (feats) {
+        w.feat = feat_.p;
+        w.hist = phist_[cur_].p;
+        w.gradrho = gradrho_.p;
+        w.mlp = warm ? reinterpret_cast<const MlpPacked*>(mlp_packed_.p) : nullptr;
+        w.p_scale = P.delta * 0.01f * P.rho0;
+        last_p_scale_ = w.p_scale;
+        features_valid_ = true;
+    }
     if (prm_.loop_mode == LSP_LOOP_PERSISTENT) {
         CK(cudaMemsetAsync(loop_sync_.p, 0, 4 * sizeof(uint32_t), stream_));
-        CK(cudaMemsetAsync(maxerr_.p, 0, (size_t)P.max_it * sizeof(uint32_t), stream_));
+        CK(cudaMemsetAsync(maxerr_.p, 0, (size_t)(P.max_it + 4) * sizeof(uint32_t), stream_));
+        if (feats) {
+            w.maxerr0 = maxerr_.p;
+            timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, 0, stream_); return 1; });
+            timed(LSP_PROF_WARM_START, [&] { launch_pci_density_first(P, b, w, stream_); return 1; });
+        }
         bool ok = false;
         int grid = 0;
         timed(LSP_PROF_PCI_LOOP, [&] {
-            ok = launch_pci_loop(P, b, ppos_alt_.p, loop_sync_.p, maxerr_.p, stream_, &grid);
+            ok = launch_pci_loop(P, b, ppos_alt_.p, loop_sync_.p, maxerr_.p, feats ? 1 : 0, warm ? 1 : 0, stream_,
+                                 &grid);
             return ok ? 1 : 0;
         });
         if (ok) return true;
-        cudaGetLastError();   // a refused cooperative launch leaves a sticky-free error; fall back
+        cudaGetLastError();   // the device refused the cooperative launch: run the per-phase loop
+        if (feats) throw Error(LSP_ERR_CUDA, "cooperative launch of the PCISPH loop was refused");
     }
-    int it = 0;
-    bool conv = false;
-    float maxErr = 0.f, ratio = 0.f;
-    for (int k = 0; k < P.max_it; k++) {
-        timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, k, stream_); return 1; });
-        timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, k, stream_); return 1; });
-        timed(LSP_PROF_PCI_FORCE, [&] { launch_pci_force(P, b, stream_); return 1; });
-        it = k + 1;
+    // Per-phase loop; the convergence test reads the iteration's maximum back every time.
+    auto read_err = [&]() {
+        float e;
         CK(cudaMemcpyAsync(&hstatus_->max_err_bits, &status_.p->max_err_bits, sizeof(uint32_t),
                            cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
-        std::memcpy(&maxErr, &hstatus_->max_err_bits, 4);
-        ratio = maxErr / prm_.rest_density;
-        conv = std::fabs(ratio) < prm_.pci_eta;
-        if (conv && it >= P.min_it) break;
+        std::memcpy(&e, &hstatus_->max_err_bits, 4);
+        return e;
+    };
+    int k = 0, passes = 1;
+    bool conv = false, rejected = false;
+    timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, 0, stream_); return 1; });
+    if (feats) {
+        w.maxerr0 = &status_.p->max_err_bits;
+        timed(LSP_PROF_WARM_START, [&] { launch_pci_density_first(P, b, w, stream_); return 1; });
+    } else {
+        timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, 0, stream_); return 1; });
+    }
+    float e = read_err(), e0 = e;
+    for (;;) {
+        if (warm && !rejected && k == 1 && e > e0) {
+            // The learned guess raised the error: restart from zero pressure (the plain loop).
+            rejected = true;
+            k = 0;
+            passes++;
+            timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, 0, stream_); return 1; });
+            timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, 0, stream_); return 1; });
+            e = read_err();
+            continue;
+        }
+        conv = std::fabs(e / prm_.rest_density) < prm_.pci_eta;
+        // A learned guess is only checked at iteration 1, so a warm step cannot stop at 0.
+        const bool unverified = warm && !rejected && k == 0;
+        const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
+        timed(LSP_PROF_PCI_FORCE, [&] { launch_pci_force(P, b, stream_); return 1; });
+        if (done) break;
+        k++;
+        passes++;
+        timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, k, stream_); return 1; });
+        timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, k, stream_); return 1; });
+        if (k == 1) e0 = e;
+        e = read_err();
     }
     if (st) {
-        st->iterations = it;
+        st->iterations = passes;
         st->converged = conv ? 1 : 0;
-        st->max_density_error_ratio = (double)maxErr / (double)prm_.rest_density;
+        st->max_density_error_ratio = (double)e / (double)prm_.rest_density;
+        st->warm_start_used = (warm && !rejected) ? 1 : 0;
     }
     return false;
 }
@@ -560,12 +653,13 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
     ensure_grid();
     if (cols_dirty_) upload_colliders();
     if (tables_dirty_) {
-        if (!tables_.p) tables_.alloc(5 * kTableSize);
-        CK(cudaMemcpyAsync(tables_.p, hk_.tables.data(), 5 * kTableSize * sizeof(float), cudaMemcpyHostToDevice,
+        if (!tables_.p) tables_.alloc(hk_.tables.size());
+        CK(cudaMemcpyAsync(tables_.p, hk_.tables.data(), hk_.tables.size() * sizeof(float), cudaMemcpyHostToDevice,
                            stream_));
         tables_dirty_ = false;
     }
     if (!dcols_.p) upload_colliders();
+    if (features_on()) ensure_warm_buffers();
     if (nbr_cap_ == 0 || nbr_stride_ < cap_) ensure_neighbors(nbr_cap_ ? nbr_cap_ : initial_neighbor_capacity(prm_));
     lsp_step_stats local{};
     bool device_loop = false;
@@ -580,6 +674,7 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         g.half_out = half_[1 - cur_].p; g.old_out = old_[1 - cur_].p;
         g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
         g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
+        g.hist_in = phist_[cur_].p; g.hist_out = phist_[1 - cur_].p;
         g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
         timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_sort(g, stream_); });
         timed(LSP_PROF_NEIGHBORS, [&] { return launch_neighbors(g, stream_); });
@@ -614,7 +709,8 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         local.iterations = hstatus_->iterations;
         local.converged = hstatus_->converged;
         local.max_density_error_ratio = (double)me / (double)prm_.rest_density;
-        ppos_final_ = ((local.iterations - 1) & 1) ? ppos_alt_.p : ppos_.p;
+        local.warm_start_used = hstatus_->warm_used;
+        ppos_final_ = (hstatus_->last_k & 1) ? ppos_alt_.p : ppos_.p;
     }
     local.max_neighbors = (int32_t)hstatus_->max_neighbors;
     local.escaped = (int32_t)hstatus_->escaped;
@@ -769,6 +865,160 @@ void Engine::read_grid(uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_s
         CK(cudaMemcpyAsync(cell_start, cell_start_.p, cells_plus_one * sizeof(uint32_t), cudaMemcpyDeviceToHost,
                            stream_));
     }
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// ------------------------------------------------------------------ learned warm start
+
+void Engine::ensure_warm_buffers()
+{
+    if (phist_[cur_].p || cap_ == 0) return;
+    activate();
+    for (int k = 0; k < 2; k++) {
+        phist_[k].alloc(cap_);
+        CK(cudaMemsetAsync(phist_[k].p, 0, cap_ * sizeof(float4), stream_));
+    }
+    feat_.alloc(cap_ * kMlpIn);
+    gradrho_.alloc(cap_);
+    tgt_.alloc(cap_);
+    CK(cudaMemsetAsync(feat_.p, 0, cap_ * kMlpIn * sizeof(float), stream_));
+    CK(cudaMemsetAsync(gradrho_.p, 0, cap_ * sizeof(float), stream_));
+}
+
+void Engine::mlp_repack()
+{
+    launch_mlp_pack(mlp_master_.p, reinterpret_cast<MlpPacked*>(mlp_packed_.p), stream_);
+    CK(cudaGetLastError());
+}
+
+// Uniform(-a, a) weights with a = sqrt(6 / (fan_in + fan_out)), zero biases, the output
+// layer scaled down so an untrained network guesses close to zero.
+void Engine::mlp_reset(uint64_t seed)
+{
+    activate();
+    std::vector<float> w(kMlpParams, 0.f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int fin, int fout, float scale) {
+        std::uniform_real_distribution<float> u(-1.f, 1.f);
+        float a = scale * std::sqrt(6.f / (float)(fin + fout));
+        for (int i = 0; i < fin * fout; i++) w[off + i] = a * u(rng);
+    };
+    fill(kOffW1, kMlpIn, kMlpHidden, 1.f);
+    fill(kOffW2, kMlpHidden, kMlpHidden, 1.f);
+    fill(kOffW3, kMlpHidden, 1, 0.1f);
+    if (!mlp_master_.p) {
+        mlp_master_.alloc(kMlpParams);
+        mlp_m1_.alloc(kMlpParams);
+        mlp_m2_.alloc(kMlpParams);
+        mlp_grad_.alloc(kMlpParams);
+        mlp_loss_.alloc(1);
+        mlp_packed_.alloc(sizeof(MlpPacked) / 4);
+    }
+    mlp_set(w.data(), kMlpParams);
+}
+
+void Engine::mlp_set(const float* w, int n)
+{
+    if (!w || n != kMlpParams) throw Error(LSP_ERR_INVALID, "MLP parameter vector must hold 1377 floats");
+    activate();
+    CK(cudaMemcpyAsync(mlp_master_.p, w, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemsetAsync(mlp_m1_.p, 0, kMlpParams * sizeof(float), stream_));
+    CK(cudaMemsetAsync(mlp_m2_.p, 0, kMlpParams * sizeof(float), stream_));
+    mlp_step_ = 0;
+    mlp_repack();
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::mlp_get(float* w, int n)
+{
+    if (!w || n != kMlpParams) throw Error(LSP_ERR_INVALID, "MLP parameter vector must hold 1377 floats");
+    activate();
+    CK(cudaMemcpyAsync(w, mlp_master_.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::mlp_record(bool on)
+{
+    record_ = on;
+    if (on) ensure_warm_buffers();
+}
+
+// Adam steps on the features and final pressures of the last step (targets p / p_scale).
+float Engine::mlp_train(int iterations, int batch, float lr, uint64_t seed)
+{
+    if (!features_valid_ || !stepped_ || n_ == 0)
+        throw Error(LSP_ERR_STATE, "mlp_train needs a PCISPH step that recorded features (lsp_mlp_record)");
+    if (iterations <= 0 || batch <= 0) throw Error(LSP_ERR_INVALID, "iterations and batch must be > 0");
+    activate();
+    batch = (int)std::min<int64_t>(batch, n_);
+    const int rows = mlp_grad_rows(batch);
+    if (mlp_partial_.n < (size_t)rows * kMlpParams) mlp_partial_.alloc((size_t)rows * kMlpParams);
+    if (mlp_loss_part_.n < (size_t)rows) mlp_loss_part_.alloc(rows);
+    if (mlp_idx_.n < (size_t)batch) mlp_idx_.alloc(batch);
+    launch_scale(pres_.p, tgt_.p, n_, 1.f / last_p_scale_, stream_);
+    for (int it = 0; it < iterations; it++) {
+        launch_random_indices(mlp_idx_.p, batch, (int)n_, seed * 1000003ull + (uint64_t)it, stream_);
+        launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), feat_.p, tgt_.p, mlp_idx_.p, batch,
+                        mlp_partial_.p, mlp_loss_part_.p, stream_);
+        mlp_step_++;
+        launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, nullptr,
+                        mlp_loss_.p, lr, mlp_step_, 1, stream_);
+        mlp_repack();
+    }
+    CK(cudaGetLastError());
+    float loss = 0.f;
+    CK(cudaMemcpyAsync(&loss, mlp_loss_.p, sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return loss / (float)batch;
+}
+
+void Engine::mlp_forward(const float* feat, int64_t n, float* out)
+{
+    if (!feat || !out || n <= 0 || n > (1 << 26)) throw Error(LSP_ERR_INVALID, "mlp_forward: bad arguments");
+    activate();
+    if (mlp_io_.n < (size_t)n * (kMlpIn + 2)) mlp_io_.alloc((size_t)n * (kMlpIn + 2));
+    float* df = mlp_io_.p;
+    float* dout = df + n * kMlpIn;
+    CK(cudaMemcpyAsync(df, feat, n * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    launch_mlp_infer(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dout, (int)n, stream_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, dout, n * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// Gradient of 1/(2n) sum (y - t)^2 over the given batch at the current parameters.
+float Engine::mlp_gradient(const float* feat, const float* target, int64_t n, float* grad)
+{
+    if (!feat || !target || !grad || n <= 0 || n > (1 << 26)) throw Error(LSP_ERR_INVALID, "mlp_gradient: bad arguments");
+    activate();
+    if (mlp_io_.n < (size_t)n * (kMlpIn + 2)) mlp_io_.alloc((size_t)n * (kMlpIn + 2));
+    float* df = mlp_io_.p;
+    float* dt = df + n * kMlpIn;
+    CK(cudaMemcpyAsync(df, feat, n * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(dt, target, n * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    const int rows = mlp_grad_rows((int)n);
+    if (mlp_partial_.n < (size_t)rows * kMlpParams) mlp_partial_.alloc((size_t)rows * kMlpParams);
+    if (mlp_loss_part_.n < (size_t)rows) mlp_loss_part_.alloc(rows);
+    launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dt, nullptr, (int)n, mlp_partial_.p,
+                    mlp_loss_part_.p, stream_);
+    launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, mlp_grad_.p,
+                    mlp_loss_.p, 0.f, 1, 0, stream_);
+    CK(cudaGetLastError());
+    float loss = 0.f;
+    CK(cudaMemcpyAsync(grad, mlp_grad_.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(&loss, mlp_loss_.p, sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return loss / (float)n;
+}
+
+void Engine::read_features(float* out, int64_t n)
+{
+    if (!out || n != n_) throw Error(LSP_ERR_INVALID, "read_features: n must equal the particle count");
+    if (!features_valid_) throw Error(LSP_ERR_STATE, "no step has recorded features");
+    activate();
+    stage((size_t)n * kMlpIn);
+    launch_gather_rows(feat_.p, kMlpIn, slot_of_id_.p, stage_.p, n, stream_);
+    CK(cudaMemcpyAsync(out, stage_.p, (size_t)n * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
 }
 

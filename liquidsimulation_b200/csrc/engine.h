@@ -77,6 +77,16 @@ public:
     void profile_read(double* ms, int64_t* launches, int capacity);
     int64_t launch_count() const { return launches_; }
 
+    // Learned warm start (lsp_mlp_*).
+    void mlp_reset(uint64_t seed);
+    void mlp_set(const float* w, int n);
+    void mlp_get(float* w, int n);
+    void mlp_record(bool on);
+    float mlp_train(int iterations, int batch, float lr, uint64_t seed);
+    void mlp_forward(const float* feat, int64_t n, float* out);
+    float mlp_gradient(const float* feat, const float* target, int64_t n, float* grad);
+    void read_features(float* out, int64_t n);
+
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
     // Device order view for in-library callers (kernel timing, the MLP).
@@ -143,6 +153,19 @@ private:
     int64_t launches_ = 0;
     DevArray<int32_t> bounds_;
     bool stepped_ = false;
+
+    // Learned warm start state.
+    bool features_on() const;
+    void ensure_warm_buffers();
+    void mlp_repack();
+    bool record_ = false, features_valid_ = false;
+    float last_p_scale_ = 1.f;
+    DevArray<float4> phist_[2];   // pressure history (p_{n-1}, p_{n-2}, p_{n-3})
+    DevArray<float> feat_, gradrho_, tgt_;
+    DevArray<float> mlp_master_, mlp_m1_, mlp_m2_, mlp_partial_, mlp_loss_part_, mlp_grad_, mlp_loss_, mlp_io_;
+    DevArray<int32_t> mlp_idx_;
+    DevArray<uint32_t> mlp_packed_;
+    int mlp_step_ = 0;
 };
 
 }  // namespace lsp

@@ -183,7 +183,8 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
                               const float4* __restrict__ ihalf, const float4* __restrict__ iold,
                               float4* __restrict__ opos, float4* __restrict__ ovel,
                               float4* __restrict__ ohalf, float4* __restrict__ oold,
-                              int32_t* __restrict__ slot_of_id, uint32_t* __restrict__ sorted_key, DevStatus* st)
+                              int32_t* __restrict__ slot_of_id, uint32_t* __restrict__ sorted_key, DevStatus* st,
+                              const float4* __restrict__ ihist, float4* __restrict__ ohist)
 {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= P.n) return;
@@ -202,6 +203,7 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
     ovel[dest] = ivel[e.x];
     ohalf[dest] = ihalf[e.x];
     oold[dest] = iold[e.x];
+    if (ohist) ohist[dest] = ihist[e.x];
     slot_of_id[e.y] = (int32_t)dest;
     sorted_key[dest] = k;
 }
@@ -286,7 +288,8 @@ int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s)
         k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
         k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
                                                        a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
-                                                       a.old_out, a.slot_of_id, a.sorted_key, a.status);
+                                                       a.old_out, a.slot_of_id, a.sorted_key, a.status, a.hist_in,
+                                                       a.hist_out);
         launches += 2;
     }
     return launches;

@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
 #include <cuda_runtime.h>
 
 namespace lsp {
@@ -44,7 +45,8 @@ struct DevStatus {
     uint32_t barrier_gen;
     uint32_t timeout_site;
     float last_ratio;
-    uint32_t pad[5];
+    int32_t last_k;             // logical index of the loop's last iteration (persistent loop)
+    uint32_t pad[4];
 };
 
 struct DevParams {
@@ -52,6 +54,7 @@ struct DevParams {
     float h;            // kernel radius = grid spacing
     float h2;           // h * h, the neighbour-test bound (SPHSpatialGrid.cpp:69)
     float step;         // table division step h / 1000 (SPHKernel.cpp:134-137)
+    float inv_step;     // 1 / step, rounded (only a first guess of the table slot)
     float radius;       // particle radius (collisions)
     float mass;
     float rho0;
@@ -103,12 +106,29 @@ __device__ __forceinline__ void normalize(V3& a)
 __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
 
 // SPHKernel::get*Weight (SPHKernel.cpp:13-44): zero at or beyond h, else the table
-// entry at trunc(d / step).
-__device__ __forceinline__ float lookup(const float* tab, float d, const DevParams& P)
+// entry at trunc(d / step), with d / step rounded as IEEE division rounds it.
+//
+// The slot is found without a division. thr[k] (kTableSize + 1 entries, built on the
+// host by bisection over floats) is the smallest distance whose IEEE quotient d / step
+// truncates to at least k, so the exact slot is the largest k with thr[k] <= d. An
+// approximate quotient d * (1 / step), rounded to the nearest integer by the magic-number
+// addition (1.5 * 2^23), lands on that slot or the one above it (its relative error is a
+// few ulp and d / step < 1001), and one comparison with thr picks the right one. The
+// clamp keeps any input, NaN included, inside the table.
+__host__ __device__ __forceinline__ int table_slot(float d, float inv_step, const float* thr)
+{
+    float r = d * inv_step + 12582912.f;
+    int32_t bits;
+    memcpy(&bits, &r, 4);
+    int k = bits - 0x4B400000;
+    k = k < 1 ? 1 : (k > kTableSize ? kTableSize : k);
+    return (d >= thr[k]) ? k : k - 1;
+}
+
+__device__ __forceinline__ float lookup(const float* tab, const float* thr, float d, const DevParams& P)
 {
     if (d >= P.h) return 0.f;
-    int key = (int)(d / P.step);
-    return tab[key];
+    return tab[table_slot(d, P.inv_step, thr)];
 }
 
 // ----------------------------------------------------------------- collisions
@@ -198,6 +218,34 @@ __device__ __forceinline__ void collide(const Collider& o, V3& pos, V3& vel, con
 __device__ __forceinline__ void collide_all(const Collider* cols, int ncoll, V3& pos, V3& vel, const DevParams& P)
 {
     for (int c = 0; c < ncoll; c++) collide(cols[c], pos, vel, P);
+}
+
+// Walks particle i's neighbour list (column-major, `stride` apart) in list order. Loads of
+// the next B indices are issued together, then the B neighbour records, and only then the
+// per-pair arithmetic f(j, record) runs, in list order: the dependent index -> record
+// loads of B pairs are in flight at once instead of one pair at a time, and every sum
+// still accumulates in the reference's order.
+template <int B, typename Load, typename F>
+__device__ __forceinline__ void for_each_neighbor(const int32_t* __restrict__ list, int64_t stride, int cnt,
+                                                  Load load, F f)
+{
+    int e = 0;
+    for (; e + B <= cnt; e += B) {
+        int j[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) j[u] = __ldg(list + u * stride);
+        list += B * stride;
+        decltype(load(0)) r[B];
+#pragma unroll
+        for (int u = 0; u < B; u++) r[u] = load(j[u]);
+#pragma unroll
+        for (int u = 0; u < B; u++) f(j[u], r[u]);
+    }
+    for (; e < cnt; e++) {
+        int jj = __ldg(list);
+        list += stride;
+        f(jj, load(jj));
+    }
 }
 
 // Cell coordinate of the reference's CPU grid (SPHSpatialGrid.cpp:80-82).

@@ -26,9 +26,23 @@ struct GridBuildArgs {
     int2* tmp;
     int32_t* slot_of_id;
     uint32_t* sorted_key;
+    const float4* hist_in;   // optional fifth persistent array (warm-start history)
+    float4* hist_out;
     int32_t* nbr;
     int32_t* nbr_count;
     DevStatus* status;
+};
+
+struct MlpPacked;
+
+// Learned warm start inputs (device order). Features of particle i: feat[8*i .. 8*i+7].
+struct WarmArgs {
+    float* feat;            // written when non-null (recording or warm start)
+    const float4* hist;     // (p_{n-1}, p_{n-2}, p_{n-3}, -) per particle
+    const float* gradrho;   // |grad rho| from the non-pressure pass
+    const MlpPacked* mlp;   // non-null: evaluate the MLP and seed p with its guess
+    float p_scale;          // pressure of one correction at 1 % density error: delta * 0.01 * rho0
+    uint32_t* maxerr0;      // max |error| of iteration 0 (float bits)
 };
 
 // Per-step particle buffers in device (sorted) order.
@@ -46,6 +60,8 @@ struct StepBuffers {
     float4* pforce;
     float* prho;
     float* err;
+    float4* hist;             // warm-start pressure history, null when off
+    float* gradrho;           // |grad rho|, null when off
     // neighbours
     const int32_t* nbr;
     const int32_t* nbr_count;
@@ -60,6 +76,7 @@ int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
 int launch_neighbors(const GridBuildArgs& a, cudaStream_t s);
 
 void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+// With b.gradrho set, also stores |grad rho| (a warm-start feature).
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 void launch_sph_pressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 void launch_integrate_collide(const DevParams& P, const StepBuffers& b, bool add_pforce, cudaStream_t s);
@@ -70,8 +87,23 @@ void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // Whole predict-correct loop in one cooperative persistent launch; returns false when the
 // device cannot co-schedule the grid (the caller then uses the per-phase launches).
 // ppos_alt: second predicted-position buffer; sync: 16 zeroed bytes; maxerr: max_it zeroed words.
+// first_done: iteration 0's predict and density already ran (launch_pci_density_first).
+// warm: iteration 0 carried a learned pressure guess, rejected at iteration 1 if it raised
+// the maximum density error (the loop then restarts from zero pressure).
 bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
-                     cudaStream_t s, int* grid_used);
+                     int first_done, int warm, cudaStream_t s, int* grid_used);
+// Iteration 0's density pass with the warm-start features (and, with w.mlp, the guess).
+void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const WarmArgs& w, cudaStream_t s);
+
+// MLP (mlp.cu).
+void launch_mlp_pack(const float* master, MlpPacked* packed, cudaStream_t s);
+void launch_mlp_infer(const MlpPacked* packed, const float* feat, float* out, int n, cudaStream_t s);
+int mlp_grad_rows(int nb);
+void launch_mlp_grad(const MlpPacked* packed, const float* feat, const float* target, const int32_t* idx, int nb,
+                     float* partial, float* loss_partial, cudaStream_t s);
+void launch_mlp_adam(const float* partial, const float* loss_partial, int rows, float* master, float* m1, float* m2,
+                     float* grad_out, float* loss_out, float lr, int step, int apply, cudaStream_t s);
+void launch_random_indices(int32_t* idx, int nb, int n, uint64_t seed, cudaStream_t s);
 
 // Gathers a per-particle field from device order into caller order.
 // comps: 1 (float) or 3 (xyz of a float4); src is float* or float4* accordingly.
@@ -90,6 +122,9 @@ void launch_gather_state(const float4* pos, const float4* vel, const float4* hve
 void launch_neighbor_export(const int32_t* nbr, const int32_t* count, int64_t stride, const float4* pos,
                             const int32_t* slot_of_id, const int64_t* offsets, int32_t* out, int64_t n,
                             cudaStream_t s);
+void launch_scale(const float* src, float* dst, int64_t n, float factor, cudaStream_t s);
+// out[id][c] = src[slot_of_id[id]][c] for rows of `width` floats.
+void launch_gather_rows(const float* src, int width, const int32_t* slot_of_id, float* out, int64_t n, cudaStream_t s);
 // Axis-aligned bounds of the positions: out[0..2] = min, out[3..5] = max (as ordered ints).
 void launch_bounds(const float4* pos, int64_t n, int32_t* out, cudaStream_t s);
 

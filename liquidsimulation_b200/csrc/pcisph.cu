@@ -6,6 +6,7 @@
 //   k_pci_force    F_p = -m rho_i sum dW(x*) (s_i + s_j) (x*_i - x*_j) / d
 #include "lsp_device.cuh"
 #include "lsp_kernels.h"
+#include "mlp.cuh"
 
 #include <algorithm>
 
@@ -13,7 +14,12 @@ namespace lsp {
 
 constexpr int kThreads = 256;
 
-enum { T_W = 0, T_SPIKY_DW = 3 };
+enum { T_W = 0, T_SPIKY_DW = 3, T_THRESH = 5 };
+
+__device__ __forceinline__ void stage_thresholds(float* sm, const float* g)
+{
+    for (int t = threadIdx.x; t < kTableSize + 1; t += blockDim.x) sm[t] = g[T_THRESH * kTableSize + t];
+}
 
 // PCISPHSolver.cpp:67-97 for one particle. Iteration 0 starts from p = 0, F_p = 0
 // (:58-62). aproximateVelocity (:96, SPHParticle.cpp:46-49) sets v = (v_half_old + v_half)/2;
@@ -50,18 +56,14 @@ __global__ void __launch_bounds__(kThreads) k_pci_predict(DevParams P, StepBuffe
 
 // PCISPHSolver.cpp:100-126 for one particle; returns |error| (0 for NaN, which the
 // reference's std::max ignores).
-__device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W, int i,
-                                                 int iteration, float4* ppos)
+__device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W,
+                                                 const float* TH, int i, int iteration, float4* ppos)
 {
     const V3 xi = v3(ppos[i]);
-    const int cnt = __ldg(b.nbr_count + i);
-    const int32_t* list = b.nbr + i;
     float sum = 0.f;
-    for (int e = 0; e < cnt; e++) {
-        int j = __ldg(list);
-        list += P.nbr_stride;
-        sum += lookup(W, mag(v3(ppos[j]) - xi), P);
-    }
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return ppos[j]; },
+                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
     float pd = P.mass * sum;
     float er = pd - P.rho0;
     float pp = P.delta * er;
@@ -83,12 +85,13 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 
 __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffers b, int iteration)
 {
-    __shared__ float W[kTableSize];
+    __shared__ float W[kTableSize], TH[kTableSize + 1];
     __shared__ float wmax[kThreads / 32];
     for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
+    stage_thresholds(TH, b.tables);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float a = i < P.n ? pci_density_one(P, b, W, i, iteration, b.ppos) : 0.f;
+    float a = i < P.n ? pci_density_one(P, b, W, TH, i, iteration, b.ppos) : 0.f;
     // Max of non-negative floats: their bit patterns order like the values.
     uint32_t m = __float_as_uint(a);
 #pragma unroll
@@ -104,25 +107,22 @@ __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffe
 
 // PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
 // reference recomputes per pair; the prefactor uses the current density rho_i.
-__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW, int i,
-                                              const float4* ppos)
+__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
+                                              const float* TH, int i, const float4* ppos)
 {
     const float4 pi4 = ppos[i];
     const V3 xi = v3(pi4);
     const float tf = pi4.w;
     V3 pf = v3(0.f, 0.f, 0.f);
-    const int cnt = __ldg(b.nbr_count + i);
-    const int32_t* list = b.nbr + i;
-    for (int e = 0; e < cnt; e++) {
-        int j = __ldg(list);
-        list += P.nbr_stride;
-        if (j == i) continue;
-        const float4 pj4 = ppos[j];
-        const V3 xj = v3(pj4);
-        float d = mag(xj - xi);
-        V3 dir = (xi - xj) / d;
-        pf += dir * lookup(SDW, d, P) * (tf + pj4.w);
-    }
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return ppos[j]; },
+                         [&](int j, float4 pj4) {
+                             if (j == i) return;
+                             const V3 xj = v3(pj4);
+                             float d = mag(xj - xi);
+                             V3 dir = (xi - xj) / d;
+                             pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
+                         });
     pf *= -(P.mass * b.rho[i]);
     if (isnan(pf.x)) pf = v3(0.f, 0.f, 0.f);
     b.pforce[i] = f4(pf, 0.f);
@@ -130,12 +130,13 @@ __device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuff
 
 __global__ void __launch_bounds__(kThreads) k_pci_force(DevParams P, StepBuffers b)
 {
-    __shared__ float SDW[kTableSize];
+    __shared__ float SDW[kTableSize], TH[kTableSize + 1];
     for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) SDW[t] = b.tables[T_SPIKY_DW * kTableSize + t];
+    stage_thresholds(TH, b.tables);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    pci_force_one(P, b, SDW, i, b.ppos);
+    pci_force_one(P, b, SDW, TH, i, b.ppos);
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
@@ -151,6 +152,120 @@ void launch_pci_density(const DevParams& P, const StepBuffers& b, int iteration,
 void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
     if (P.n) k_pci_force<<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+}
+
+// ------------------------------------------------------------------ learned warm start
+//
+// Features of particle i at iteration 0 (all dimensionless):
+//   f0 predicted density error at zero pressure, in % of rho0 (clamped to +-50)
+//   f1 f2 f3  pressures of the previous three steps / p_scale
+//   f4 neighbour count / 32      f5 |v| dt / h * 10      f6 |grad rho| h / rho0
+//   f7 distance to the nearest collider surface / (4 h), clamped to [0, 1]
+// p_scale = delta * 0.01 * rho0 is the pressure one correction assigns to a 1 % error.
+
+__device__ __forceinline__ float collider_distance(const Collider& o, V3 x)
+{
+    V3 d = v3(fabsf(x.x - o.cx), fabsf(x.y - o.cy), fabsf(x.z - o.cz));
+    if (o.sphere) {
+        float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
+        return o.boundary ? o.radius - r : r - o.radius;
+    }
+    if (o.boundary) return fminf(fminf(o.hx - d.x, o.hy - d.y), o.hz - d.z);
+    return fmaxf(fmaxf(d.x - o.hx, d.y - o.hy), d.z - o.hz);
+}
+
+__device__ __forceinline__ void warm_features(const DevParams& P, const StepBuffers& b, const WarmArgs& w, int i,
+                                              float pd, int cnt, float (&f)[kMlpIn])
+{
+    const float4 hs = w.hist[i];
+    const float4 v = b.vel[i];
+    const V3 x = v3(b.pos[i]);
+    f[0] = fminf(fmaxf((pd - P.rho0) / (0.01f * P.rho0), -50.f), 50.f);
+    f[1] = hs.x / w.p_scale;
+    f[2] = hs.y / w.p_scale;
+    f[3] = hs.z / w.p_scale;
+    f[4] = (float)cnt * (1.f / 32.f);
+    f[5] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * P.dt / P.h * 10.f;
+    f[6] = w.gradrho[i] * P.h / P.rho0;
+    float dist = 4.f * P.h;
+    for (int c = 0; c < P.ncoll; c++) dist = fminf(dist, fmaxf(collider_distance(b.colliders[c], x), 0.f));
+    f[7] = dist / (4.f * P.h);
+}
+
+// Iteration 0's density pass (PCISPHSolver.cpp:100-126 with p starting at 0) that also
+// computes the warm-start features and, with w.mlp, replaces the pressure of this first
+// correction by the network's guess. Without w.mlp its results are those of the plain pass.
+__global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, StepBuffers b, WarmArgs w)
+{
+    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ MlpPacked mw;
+    __shared__ uint32_t stage[kThreads / 32][32 * 4];
+    __shared__ float wmax[kThreads / 32];
+    for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
+    stage_thresholds(TH, b.tables);
+    if (w.mlp) {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(w.mlp);
+        uint32_t* dst = reinterpret_cast<uint32_t*>(&mw);
+        for (int t = threadIdx.x; t < (int)(sizeof(MlpPacked) / 4); t += blockDim.x) dst[t] = src[t];
+    }
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    float a = 0.f, pd = 0.f, p = 0.f;
+    float f[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (valid) {
+        const V3 xi = v3(b.ppos[i]);
+        const int cnt = __ldg(b.nbr_count + i);
+        float sum = 0.f;
+        for_each_neighbor<4>(b.nbr + i, P.nbr_stride, cnt, [&](int j) { return b.ppos[j]; },
+                             [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+        pd = P.mass * sum;
+        float er = pd - P.rho0;
+        float pp = P.delta * er;
+        if (pp < 0.f) {
+            er *= P.neg;
+            pp *= P.neg;
+        }
+        p = 0.f + pp;
+        b.prho[i] = pd;
+        b.err[i] = er;
+        a = fabsf(er);
+        a = a == a ? a : 0.f;
+        warm_features(P, b, w, i, pd, cnt, f);
+        if (w.feat) {
+#pragma unroll
+            for (int c = 0; c < kMlpIn; c++) w.feat[(int64_t)i * kMlpIn + c] = f[c];
+        }
+    }
+    if (w.mlp) {
+        float y = mlp_warp_eval(mw, f, stage[threadIdx.x >> 5]);
+        if (valid) {
+            p = y * w.p_scale;
+            if (P.neg == 0.f && p < 0.f) p = 0.f;
+        }
+    }
+    if (valid) {
+        b.pres[i] = p;
+        reinterpret_cast<float*>(b.ppos + i)[3] = p / (pd * pd);
+    }
+    uint32_t m = __float_as_uint(a);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = __uint_as_float(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t bm = 0;
+        for (int k = 0; k < kThreads / 32; k++) bm = max(bm, __float_as_uint(wmax[k]));
+        if (bm) {
+            atomicMax(w.maxerr0, bm);
+            atomicMax(&b.status->max_err_bits, bm);
+        }
+    }
+}
+
+void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const WarmArgs& w, cudaStream_t s)
+{
+    if (P.n) k_pci_density_first<<<(unsigned)((P.n + kThreads - 1) / kThreads), kThreads, 0, s>>>(P, b, w);
 }
 
 // ------------------------------------------------------------------ persistent loop
@@ -217,25 +332,24 @@ __device__ bool grid_barrier(LoopSync* sy, DevStatus* st)
 }
 
 __global__ void __launch_bounds__(kThreads) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt, LoopSync* sy,
-                                                      uint32_t* maxerr)
+                                                      uint32_t* maxerr, int first_done, int warm)
 {
-    __shared__ float W[kTableSize], SDW[kTableSize];
+    __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1];
     __shared__ float wmax[kThreads / 32];
     for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) {
         W[t] = b.tables[T_W * kTableSize + t];
         SDW[t] = b.tables[T_SPIKY_DW * kTableSize + t];
     }
+    stage_thresholds(TH, b.tables);
     __syncthreads();
     float4* pp[2] = {b.ppos, ppos_alt};
     const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    for (int i = tid; i < P.n; i += stride) pci_predict_one(P, b, i, 0, pp[0]);
-    int k = 0;
-    bool conv = false, done = false;
-    for (k = 0; k < P.max_it; k++) {
-        if (!grid_barrier(sy, b.status)) return;
+
+    // density(k) over all particles; the block maximum of |error| goes to maxerr[slot].
+    auto density_pass = [&](int k, int slot) {
         float m = 0.f;
-        for (int i = tid; i < P.n; i += stride) m = fmaxf(m, pci_density_one(P, b, W, i, k, pp[k & 1]));
+        for (int i = tid; i < P.n; i += stride) m = fmaxf(m, pci_density_one(P, b, W, TH, i, k, pp[k & 1]));
         uint32_t mb = __float_as_uint(m);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, off));
@@ -244,25 +358,55 @@ __global__ void __launch_bounds__(kThreads) k_pci_loop(DevParams P, StepBuffers 
         if (threadIdx.x == 0) {
             uint32_t bm = 0;
             for (int w = 0; w < kThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
-            if (bm) atomicMax(&maxerr[k], bm);
+            if (bm) atomicMax(&maxerr[slot], bm);
         }
+        __syncthreads();
+    };
+
+    int k = 0, kp = 0;
+    bool conv = false, rejected = false;
+    if (!first_done) {
+        for (int i = tid; i < P.n; i += stride) pci_predict_one(P, b, i, 0, pp[0]);
         if (!grid_barrier(sy, b.status)) return;
+        density_pass(0, 0);
+        if (!grid_barrier(sy, b.status)) return;
+    }
+    for (;;) {
+        const float me = __uint_as_float(ld_volatile(&maxerr[kp]));
+        if (warm && !rejected && k == 1 && me > __uint_as_float(ld_volatile(&maxerr[kp - 1]))) {
+            // The learned guess raised the error: restart from zero pressure (the plain loop).
+            rejected = true;
+            k = 0;
+            kp++;
+            for (int i = tid; i < P.n; i += stride) pci_predict_one(P, b, i, 0, pp[0]);
+            if (!grid_barrier(sy, b.status)) return;
+            density_pass(0, kp);
+            if (!grid_barrier(sy, b.status)) return;
+            continue;
+        }
         // PCISPHSolver.cpp:152-162: ratio = max|e| / rho0 in float, exit when below eta.
-        const float me = __uint_as_float(ld_volatile(&maxerr[k]));
         const float ratio = me / P.rho0;
         conv = fabsf(ratio) < P.eta;
-        done = (conv && k + 1 >= P.min_it) || (k + 1 >= P.max_it);
+        // A learned guess is only checked at iteration 1, so a warm step cannot stop at 0.
+        const bool unverified = warm && !rejected && k == 0;
+        const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
         for (int i = tid; i < P.n; i += stride) {
-            pci_force_one(P, b, SDW, i, pp[k & 1]);
+            pci_force_one(P, b, SDW, TH, i, pp[k & 1]);
             if (!done) pci_predict_one(P, b, i, k + 1, pp[(k + 1) & 1]);
         }
         if (done) break;
+        if (!grid_barrier(sy, b.status)) return;
+        k++;
+        kp++;
+        density_pass(k, kp);
+        if (!grid_barrier(sy, b.status)) return;
     }
     if (tid == 0) {
-        int it = k < P.max_it ? k + 1 : P.max_it;
-        b.status->iterations = it;
+        b.status->iterations = kp + 1;
         b.status->converged = conv ? 1 : 0;
-        b.status->max_err_bits = it > 0 ? ld_volatile(&maxerr[it - 1]) : 0u;
+        b.status->max_err_bits = ld_volatile(&maxerr[kp]);
+        b.status->warm_used = (warm && !rejected) ? 1 : 0;
+        b.status->last_k = k;
     }
 }
 
@@ -270,7 +414,7 @@ static int g_loop_blocks_per_sm = -1;
 static int g_sm_count = 0;
 
 bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
-                     cudaStream_t s, int* grid_used)
+                     int first_done, int warm, cudaStream_t s, int* grid_used)
 {
     if (grid_used) *grid_used = 0;
     if (P.n <= 0 || P.max_it <= 0) return false;
@@ -291,7 +435,7 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     DevParams Pc = P;
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;
-    void* args[] = {&Pc, &bc, &ppos_alt, &sy, &maxerr};
+    void* args[] = {&Pc, &bc, &ppos_alt, &sy, &maxerr, &first_done, &warm};
     if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(kThreads), args, 0, s) != cudaSuccess)
         return false;
     if (grid_used) *grid_used = grid;

@@ -12,28 +12,28 @@ namespace lsp {
 
 constexpr int kThreads = 256;
 
-enum { T_W = 0, T_DW = 1, T_D2W = 2, T_SPIKY_DW = 3, T_VISC_D2W = 4 };
+enum { T_W = 0, T_DW = 1, T_D2W = 2, T_SPIKY_DW = 3, T_VISC_D2W = 4, T_THRESH = 5 };
 
 __device__ __forceinline__ void stage_table(float* sm, const float* g, int t)
 {
-    for (int i = threadIdx.x; i < kTableSize; i += blockDim.x) sm[i] = g[t * kTableSize + i];
+    const int len = t == T_THRESH ? kTableSize + 1 : kTableSize;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[t * kTableSize + i];
 }
 
 // SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
 __global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b)
 {
-    __shared__ float W[kTableSize];
+    __shared__ float W[kTableSize], TH[kTableSize + 1];
     stage_table(W, b.tables, T_W);
+    stage_table(TH, b.tables, T_THRESH);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     const V3 xi = v3(b.pos[i]);
-    const int cnt = b.nbr_count[i];
     float sum = 0.f;
-    for (int e = 0; e < cnt; e++) {
-        int j = b.nbr[(int64_t)e * P.nbr_stride + i];
-        sum += lookup(W, mag(v3(b.pos[j]) - xi), P);
-    }
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return b.pos[j]; },
+                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
     float rho = P.mass * sum;
     float pr = P.stiffness * (rho - P.rho0);
     if (pr < 0.f) pr *= P.neg;
@@ -45,9 +45,11 @@ __global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b
 // reference walks the list up to three times (normal, colour Laplacian when the normal
 // exceeds the threshold, viscosity); each sum is independent, so one walk computes all
 // three with the same per-sum rounding.
+template <bool kGrad>
 __global__ void __launch_bounds__(kThreads) k_nonpressure(DevParams P, StepBuffers b)
 {
-    __shared__ float DW[kTableSize], D2W[kTableSize], VD2W[kTableSize];
+    __shared__ float DW[kTableSize], D2W[kTableSize], VD2W[kTableSize], TH[kTableSize + 1];
+    stage_table(TH, b.tables, T_THRESH);
     stage_table(DW, b.tables, T_DW);
     stage_table(D2W, b.tables, T_D2W);
     stage_table(VD2W, b.tables, T_VISC_D2W);
@@ -62,17 +64,23 @@ __global__ void __launch_bounds__(kThreads) k_nonpressure(DevParams P, StepBuffe
     V3 normal = v3(0.f, 0.f, 0.f);
     V3 visc = v3(0.f, 0.f, 0.f);
     float lap = 0.f;
-    const int cnt = b.nbr_count[i];
-    for (int e = 0; e < cnt; e++) {
-        int j = b.nbr[(int64_t)e * P.nbr_stride + i];
-        const V3 xj = v3(b.pos[j]);
-        const float rhoj = b.rho[j];
-        V3 dir = xi - xj;
-        float d = mag(xj - xi);
-        normal += dir * lookup(DW, d, P) / rhoj;
-        lap += lookup(D2W, d, P) / rhoj;
-        if (j != i) visc += ((v3(b.vel[j]) - vi) / rhoj) * lookup(VD2W, d, P);
-    }
+    V3 grad = v3(0.f, 0.f, 0.f);   // sum (rho_j - rho_i) / rho_j grad W_ij: a warm-start feature only
+    struct Rec {
+        float4 x, v;
+        float rho;
+    };
+    for_each_neighbor<2>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return Rec{b.pos[j], b.vel[j], b.rho[j]}; },
+                         [&](int j, const Rec& r) {
+                             const V3 xj = v3(r.x);
+                             V3 dir = xi - xj;
+                             float d = mag(xj - xi);
+                             normal += dir * lookup(DW, TH, d, P) / r.rho;
+                             lap += lookup(D2W, TH, d, P) / r.rho;
+                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * lookup(VD2W, TH, d, P);
+                             if (kGrad) grad += dir * (lookup(DW, TH, d, P) * ((r.rho - rhoi) / r.rho));
+                         });
+    if (kGrad) b.gradrho[i] = P.mass * mag(grad);
     normal *= P.mass;
     float len = mag(normal);
     if (len > P.sigma_thr) F += (normal / len) * (-P.sigma * lap * P.mass);
@@ -84,8 +92,9 @@ __global__ void __launch_bounds__(kThreads) k_nonpressure(DevParams P, StepBuffe
 // SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
 __global__ void __launch_bounds__(kThreads) k_sph_pressure(DevParams P, StepBuffers b)
 {
-    __shared__ float SDW[kTableSize];
+    __shared__ float SDW[kTableSize], TH[kTableSize + 1];
     stage_table(SDW, b.tables, T_SPIKY_DW);
+    stage_table(TH, b.tables, T_THRESH);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
@@ -93,16 +102,19 @@ __global__ void __launch_bounds__(kThreads) k_sph_pressure(DevParams P, StepBuff
     const float rhoi = b.rho[i];
     const float tf = b.pres[i] / (rhoi * rhoi);
     V3 pf = v3(0.f, 0.f, 0.f);
-    const int cnt = b.nbr_count[i];
-    for (int e = 0; e < cnt; e++) {
-        int j = b.nbr[(int64_t)e * P.nbr_stride + i];
-        if (j == i) continue;
-        const V3 xj = v3(b.pos[j]);
-        const float rhoj = b.rho[j];
-        float d = mag(xi - xj);
-        V3 dir = (xi - xj) / d;
-        pf += dir * lookup(SDW, d, P) * (tf + b.pres[j] / (rhoj * rhoj));
-    }
+    struct Rec {
+        float4 x;
+        float rho, p;
+    };
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return Rec{b.pos[j], b.rho[j], b.pres[j]}; },
+                         [&](int j, const Rec& r) {
+                             if (j == i) return;
+                             const V3 xj = v3(r.x);
+                             float d = mag(xi - xj);
+                             V3 dir = (xi - xj) / d;
+                             pf += dir * lookup(SDW, TH, d, P) * (tf + r.p / (r.rho * r.rho));
+                         });
     pf *= -(P.mass * rhoi);
     V3 F = v3(b.force[i]);
     F += pf;
@@ -137,6 +149,11 @@ __global__ void __launch_bounds__(kThreads) k_integrate_collide(DevParams P, Ste
     b.vel[i] = f4(v, first);
     b.half[i] = f4(half, h4.w);
     b.old[i] = f4(old, o4.w);
+    if (b.hist) {
+        // Warm-start pressure history: (p_n, p_{n-1}, p_{n-2}) for the next step's features.
+        float4 hs = b.hist[i];
+        b.hist[i] = make_float4(b.pres[i], hs.x, hs.y, 0.f);
+    }
 }
 
 static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
@@ -147,7 +164,11 @@ void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 }
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
-    if (P.n) k_nonpressure<<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+    if (!P.n) return;
+    if (b.gradrho)
+        k_nonpressure<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+    else
+        k_nonpressure<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
 }
 void launch_sph_pressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {

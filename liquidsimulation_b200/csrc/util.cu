@@ -138,6 +138,31 @@ void launch_neighbor_export(const int32_t* nbr, const int32_t* count, int64_t st
     if (n) k_neighbor_export<<<blocks_for(n), kThreads, 0, s>>>(nbr, count, stride, pos, slot_of_id, offsets, out, n);
 }
 
+__global__ void k_scale(const float* __restrict__ src, float* __restrict__ dst, int64_t n, float f)
+{
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i] * f;
+}
+
+void launch_scale(const float* src, float* dst, int64_t n, float factor, cudaStream_t s)
+{
+    if (n) k_scale<<<blocks_for(n), kThreads, 0, s>>>(src, dst, n, factor);
+}
+
+__global__ void k_gather_rows(const float* __restrict__ src, int width, const int32_t* __restrict__ slot_of_id,
+                              float* __restrict__ out, int64_t n)
+{
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    const int64_t s = slot_of_id[id];
+    for (int c = 0; c < width; c++) out[id * width + c] = src[s * width + c];
+}
+
+void launch_gather_rows(const float* src, int width, const int32_t* slot_of_id, float* out, int64_t n, cudaStream_t s)
+{
+    if (n) k_gather_rows<<<blocks_for(n), kThreads, 0, s>>>(src, width, slot_of_id, out, n);
+}
+
 // Float min/max through order-preserving integer images (atomicMin/Max on ints).
 __device__ __forceinline__ int32_t ordered(float f)
 {

@@ -65,8 +65,9 @@ def lattice(lo, counts, s, seed, jitter=0.01, rng=None, first=None):
     return pts.astype(np.float32)
 
 
-def wall_lattice(lo, counts, s, seed, rng=None):
-    """A block resting in a corner of the walls at ``lo``: its first layer sits one particle
+def wall_lattice(lo, counts, s, seed, rng=None, hi=None):
+    """A block resting in a corner of the walls at ``lo`` (walls up to ``hi``, if given: the
+    block is clipped to fit them): its first layer sits one particle
     radius (s / 1.6) plus the jitter amplitude from each wall, so the boundary collision
     (which keeps particles r inside, StaticCollisionBox.cpp:77-114) does not move it. A
     block starting at lo + s/2 would have its first layer pinned 1/8 spacing inward by the
@@ -74,6 +75,10 @@ def wall_lattice(lo, counts, s, seed, rng=None):
     PCISPH loop run to its iteration cap."""
     off = s / 1.6 + 0.01 * s
     first = tuple(float(l) + off for l in lo)
+    if hi is not None:
+        # Layers that would fall inside the far walls' margin are dropped.
+        counts = [min(int(c), int(math.floor((float(u) - off - f) / s + 1e-9)) + 1)
+                  for c, f, u in zip(counts, first, hi)]
     return lattice(lo, counts, s, seed, rng=rng, first=first)
 
 
@@ -101,7 +106,7 @@ def dam_break_sph(seed: int = 1, scale: float = 1.0) -> Scene:
     mass 0.008, h = 0.04, k = 3, mu = 0.1, dt = 0.002. ``scale`` < 1 shrinks the block."""
     s = 0.02
     counts = [max(2, int(round(c * scale))) for c in (20, 30, 20)]
-    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed, hi=(1.0, 1.0, 1.0))
     p = _params(s, abi.LSP_SOLVER_SPH, mass_override=0.008)
     box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
     return Scene("dam_break_sph_12k", p, pos, np.zeros_like(pos), [box], 0.002, 1000,
@@ -111,22 +116,23 @@ def dam_break_sph(seed: int = 1, scale: float = 1.0) -> Scene:
 def dam_break_pcisph(seed: int = 2, counts=(64, 102, 64), s: float = 0.00625) -> Scene:
     """PCISPH dam break: unit box walls, 64x102x64 block at s = 0.00625 (417,792 particles),
     h = 2 s, eta = 1 %, min 3 / max 50 iterations, zero initial pressure, dt = 0.001."""
-    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed, hi=(1.0, 1.0, 1.0))
     p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
     box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
-    n = int(np.prod(counts))
+    n = pos.shape[0]
     return Scene(f"dam_break_pcisph_{n}", p, pos, np.zeros_like(pos), [box], 0.001, 2000,
                  domain=((0.0, 0.0, 0.0), (1.0, 1.0, 1.0)), spacing=s)
 
 
 def wave_breaker(seed: int = 3, s: float = 0.00735, block=(0.8, 0.5, 1.0)) -> Scene:
     """PCISPH wave breaker, ~1M particles: 2x1x1 walls, block [0,0.8]x[0,0.5]x[0,1] at
-    s = 0.00735 (108x68x136 = 998,784 particles); two 0.2x0.3x0.2 box obstacles and a
+    s = 0.00735 (108x68x135 = 991,440 particles: the block spans the full depth, so one
+    layer is dropped to clear the far wall's margin); two 0.2x0.3x0.2 box obstacles and a
     r = 0.15 sphere obstacle resting on the floor at seeded x in [1, 1.8]; eta = 1 %,
     min 3 / max 50, dt = 0.0008."""
     rng = np.random.Generator(np.random.PCG64(seed))
     counts = [int(math.floor(b / s + 1e-9)) for b in block]
-    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed, rng=rng)
+    pos = wall_lattice((0.0, 0.0, 0.0), counts, s, seed, rng=rng, hi=(2.0, 1.0, 1.0))
     p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
     cols = [Collider("box", (1.0, 0.5, 0.5), (1.0, 0.5, 0.5), True)]
     for _ in range(2):
@@ -150,7 +156,7 @@ def batched_dam_breaks(seed: int = 4, scenes: int = 64, nmin: int = 2000, nmax: 
         edges = rng.uniform(0.2, 0.6, size=3)
         s = float((np.prod(edges) / n_target) ** (1.0 / 3.0))
         counts = [max(2, int(e / s)) for e in edges]
-        pos = wall_lattice((0.0, 0.0, 0.0), counts, s, int(rng.integers(1 << 30)))
+        pos = wall_lattice((0.0, 0.0, 0.0), counts, s, int(rng.integers(1 << 30)), hi=(1.0, 1.0, 1.0))
         p = _params(s, abi.LSP_SOLVER_PCISPH, pci_eta=0.01, pci_min_iterations=3, pci_max_iterations=50)
         box = Collider("box", (0.5, 0.5, 0.5), (0.5, 0.5, 0.5), True)
         out.append(Scene(f"batch_{b}", p, pos, np.zeros_like(pos), [box], 0.001, 100,

@@ -233,6 +233,43 @@ class SPHSolver:
         self._call("lsp_read_neighbors", _ptr(off, POINTER(c_int64)), _ptr(idx, POINTER(c_int32)), n, idx.size)
         return off, idx[: int(off[-1])]
 
+    # ------------------------------------------------------------ learned warm start
+    def mlp_reset(self, seed: int = 0):
+        self._call("lsp_mlp_reset", ctypes.c_uint64(seed))
+
+    def mlp_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32).reshape(-1)
+        self._call("lsp_mlp_set_weights", _ptr(w), w.size)
+
+    def mlp_get_weights(self) -> np.ndarray:
+        w = np.empty(abi.MLP_PARAMS, np.float32)
+        self._call("lsp_mlp_get_weights", _ptr(w), w.size)
+        return w
+
+    def mlp_record(self, on: bool = True):
+        self._call("lsp_mlp_record", 1 if on else 0)
+
+    def mlp_train(self, iterations: int = 4, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> float:
+        """Adam steps on the last recorded step (features -> final pressure); returns the loss."""
+        loss = c_float()
+        self._call("lsp_mlp_train", int(iterations), int(batch), c_float(lr), ctypes.c_uint64(seed), byref(loss))
+        return loss.value
+
+    def mlp_forward(self, features) -> np.ndarray:
+        x = np.ascontiguousarray(features, np.float32).reshape(-1, abi.MLP_FEATURES)
+        out = np.empty(x.shape[0], np.float32)
+        self._call("lsp_mlp_forward", _ptr(x), x.shape[0], _ptr(out))
+        return out
+
+    def read_features(self) -> np.ndarray:
+        n = self.get_particle_count()
+        out = np.empty((n, abi.MLP_FEATURES), np.float32)
+        self._call("lsp_read_features", _ptr(out), n)
+        return out
+
+    def set_warm_start(self, mode: int):
+        self.set_params(warm_start=int(mode))
+
     def grid(self):
         """(dims, origin, sorted keys, sorted caller ids, dense cell table) of the last step."""
         n = self.get_particle_count()

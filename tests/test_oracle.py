@@ -117,7 +117,9 @@ def test_scene_sizes_and_determinism():
     assert scenes.dam_break_sph().n == 12000
     assert scenes.dam_break_pcisph(counts=(64, 102, 64)).n == 417792
     wb = scenes.wave_breaker()
-    assert wb.n == 108 * 68 * 136 == 998784
+    assert wb.n == 108 * 68 * 135 == 991440
+    r = wb.params.particle_radius
+    assert wb.positions.min() > r and wb.positions[:, 2].max() < 1.0 - r
     a = scenes.small_box_scene(seed=3).positions
     b = scenes.small_box_scene(seed=3).positions
     assert np.array_equal(a, b)
