@@ -189,6 +189,10 @@ int lsp_mlp_set_weights(lsp_solver* s, const float* w, int n);
 int lsp_mlp_get_weights(lsp_solver* s, float* w, int n);
 /* Records the 8 features of every particle at iteration 0 of each PCISPH step. */
 int lsp_mlp_record(lsp_solver* s, int enable);
+/* Training loss 1/(2n) sum w r^2, r = guess - target, w = over_weight when r > 0
+ * (default 1, plain MSE). PCISPH with a zero negative-pressure factor only adds pressure
+ * within a step, so over-estimates cost iterations that under-estimates do not. */
+int lsp_mlp_set_loss_asymmetry(lsp_solver* s, float over_weight);
 /* Adam steps on the last recorded step: features -> final pressure (normalised).
  * Each iteration draws `batch` random particles. loss (may be NULL): mean 0.5 (y - t)^2. */
 int lsp_mlp_train(lsp_solver* s, int iterations, int batch, float learning_rate, uint64_t seed, float* loss);

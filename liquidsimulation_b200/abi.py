@@ -215,6 +215,7 @@ def _declare(lib):
         "lsp_mlp_set_weights": (c_int, [S, fp, c_int]),
         "lsp_mlp_get_weights": (c_int, [S, fp, c_int]),
         "lsp_mlp_record": (c_int, [S, c_int]),
+        "lsp_mlp_set_loss_asymmetry": (c_int, [S, c_float]),
         "lsp_mlp_train": (c_int, [S, c_int, c_int, c_float, ctypes.c_uint64, fp]),
         "lsp_mlp_forward": (c_int, [S, fp, c_int64, fp]),
         "lsp_mlp_gradient": (c_int, [S, fp, fp, c_int64, fp, fp]),

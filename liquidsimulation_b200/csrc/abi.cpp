@@ -6,10 +6,7 @@
 
 #include "../../include/lsp.h"
 #include "engine.h"
-
-struct lsp_solver {
-    lsp::Engine* e;
-};
+#include "lsp_handle.h"
 
 namespace {
 thread_local std::string g_last_error;
@@ -47,6 +44,10 @@ void need(const void* p, const char* what)
     if (!p) throw lsp::Error(LSP_ERR_INVALID, std::string("null pointer: ") + what);
 }
 }  // namespace
+
+namespace lsp {
+void set_last_error(const std::string& message) { g_last_error = message; }
+}  // namespace lsp
 
 extern "C" {
 
@@ -286,6 +287,10 @@ int lsp_mlp_get_weights(lsp_solver* s, float* w, int n)
 int lsp_mlp_record(lsp_solver* s, int enable)
 {
     return guard([&] { E(s).mlp_record(enable != 0); });
+}
+int lsp_mlp_set_loss_asymmetry(lsp_solver* s, float over_weight)
+{
+    return guard([&] { E(s).mlp_set_loss_asymmetry(over_weight); });
 }
 int lsp_mlp_train(lsp_solver* s, int iterations, int batch, float learning_rate, uint64_t seed, float* loss)
 {

@@ -937,6 +937,15 @@ void Engine::mlp_get(float* w, int n)
     CK(cudaStreamSynchronize(stream_));
 }
 
+// Weight of the squared error of over-estimates in training. With a zero negative-pressure
+// factor PCISPH only ever adds pressure, so a guess that is too high cannot be corrected
+// within the step; weighting those errors up biases the guess low.
+void Engine::mlp_set_loss_asymmetry(float w)
+{
+    if (!(w >= 1.f) || !std::isfinite(w)) throw Error(LSP_ERR_INVALID, "loss asymmetry must be >= 1");
+    mlp_over_weight_ = w;
+}
+
 void Engine::mlp_record(bool on)
 {
     record_ = on;
@@ -959,7 +968,7 @@ float Engine::mlp_train(int iterations, int batch, float lr, uint64_t seed)
     for (int it = 0; it < iterations; it++) {
         launch_random_indices(mlp_idx_.p, batch, (int)n_, seed * 1000003ull + (uint64_t)it, stream_);
         launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), feat_.p, tgt_.p, mlp_idx_.p, batch,
-                        mlp_partial_.p, mlp_loss_part_.p, stream_);
+                        mlp_over_weight_, mlp_partial_.p, mlp_loss_part_.p, stream_);
         mlp_step_++;
         launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, nullptr,
                         mlp_loss_.p, lr, mlp_step_, 1, stream_);
@@ -999,8 +1008,8 @@ float Engine::mlp_gradient(const float* feat, const float* target, int64_t n, fl
     const int rows = mlp_grad_rows((int)n);
     if (mlp_partial_.n < (size_t)rows * kMlpParams) mlp_partial_.alloc((size_t)rows * kMlpParams);
     if (mlp_loss_part_.n < (size_t)rows) mlp_loss_part_.alloc(rows);
-    launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dt, nullptr, (int)n, mlp_partial_.p,
-                    mlp_loss_part_.p, stream_);
+    launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dt, nullptr, (int)n, 1.f,
+                    mlp_partial_.p, mlp_loss_part_.p, stream_);
     launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, mlp_grad_.p,
                     mlp_loss_.p, 0.f, 1, 0, stream_);
     CK(cudaGetLastError());

@@ -82,10 +82,14 @@ public:
     void mlp_set(const float* w, int n);
     void mlp_get(float* w, int n);
     void mlp_record(bool on);
+    void mlp_set_loss_asymmetry(float w);
     float mlp_train(int iterations, int batch, float lr, uint64_t seed);
     void mlp_forward(const float* feat, int64_t n, float* out);
     float mlp_gradient(const float* feat, const float* target, int64_t n, float* grad);
     void read_features(float* out, int64_t n);
+
+    // Device copy of the fragment-ordered MLP weights (MlpPacked).
+    const void* mlp_packed_device() const { return mlp_packed_.p; }
 
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
@@ -166,6 +170,7 @@ private:
     DevArray<int32_t> mlp_idx_;
     DevArray<uint32_t> mlp_packed_;
     int mlp_step_ = 0;
+    float mlp_over_weight_ = 1.f;
 };
 
 }  // namespace lsp

@@ -100,7 +100,10 @@ void launch_mlp_pack(const float* master, MlpPacked* packed, cudaStream_t s);
 void launch_mlp_infer(const MlpPacked* packed, const float* feat, float* out, int n, cudaStream_t s);
 int mlp_grad_rows(int nb);
 void launch_mlp_grad(const MlpPacked* packed, const float* feat, const float* target, const int32_t* idx, int nb,
-                     float* partial, float* loss_partial, cudaStream_t s);
+                     float over_weight, float* partial, float* loss_partial, cudaStream_t s);
+// k_mlp_grad on exactly `blocks` blocks of 256 threads: writes blocks * 8 partial rows.
+void launch_mlp_grad_blocks(const MlpPacked* packed, const float* feat, const float* target, int nb, int blocks,
+                            float* partial, float* loss_partial, cudaStream_t s);
 void launch_mlp_adam(const float* partial, const float* loss_partial, int rows, float* master, float* m1, float* m2,
                      float* grad_out, float* loss_out, float lr, int step, int apply, cudaStream_t s);
 void launch_random_indices(int32_t* idx, int nb, int n, uint64_t seed, cudaStream_t s);

@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const MlpPacked* __res
                                                          const float* __restrict__ feat,
                                                          const float* __restrict__ target,
                                                          const int32_t* __restrict__ idx, int nb, float inv_batch,
-                                                         float* __restrict__ partial, float* __restrict__ loss_partial)
+                                                         float over_w, float* __restrict__ partial,
+                                                         float* __restrict__ loss_partial)
 {
     __shared__ MlpPacked w;
     __shared__ uint32_t stage[kMlpWarps][32 * 4];
@@ -155,10 +156,13 @@ __global__ void __launch_bounds__(kMlpThreads) k_mlp_grad(const MlpPacked* __res
             const float t0 = __shfl_sync(0xffffffffu, tgt, 16 * m + g);
             const float t1 = __shfl_sync(0xffffffffu, tgt, 16 * m + g + 8);
             const bool v0 = base + 16 * m + g < nb, v1 = base + 16 * m + g + 8 < nb;
-            float dy0 = v0 ? (y[0] - t0) * inv_batch : 0.f;
-            float dy1 = v1 ? (y[1] - t1) * inv_batch : 0.f;
+            // Loss 1/(2n) sum w(r) r^2 with r = y - t, w = over_w when the guess is too high.
+            const float r0 = y[0] - t0, r1 = y[1] - t1;
+            const float w0 = r0 > 0.f ? over_w : 1.f, w1 = r1 > 0.f ? over_w : 1.f;
+            float dy0 = v0 ? w0 * r0 * inv_batch : 0.f;
+            float dy1 = v1 ? w1 * r1 * inv_batch : 0.f;
             if (q == 0) {
-                loss += (v0 ? 0.5f * (y[0] - t0) * (y[0] - t0) : 0.f) + (v1 ? 0.5f * (y[1] - t1) * (y[1] - t1) : 0.f);
+                loss += (v0 ? 0.5f * w0 * r0 * r0 : 0.f) + (v1 ? 0.5f * w1 * r1 * r1 : 0.f);
                 db3 += dy0 + dy1;
             }
             dy0 = __shfl_sync(0xffffffffu, dy0, 4 * g);
@@ -353,11 +357,18 @@ int mlp_grad_rows(int nb)
 }
 
 void launch_mlp_grad(const MlpPacked* packed, const float* feat, const float* target, const int32_t* idx, int nb,
-                     float* partial, float* loss_partial, cudaStream_t s)
+                     float over_weight, float* partial, float* loss_partial, cudaStream_t s)
 {
     int rows = mlp_grad_rows(nb);
-    k_mlp_grad<<<rows / kMlpWarps, kMlpThreads, 0, s>>>(packed, feat, target, idx, nb, 1.f / (float)nb, partial,
-                                                         loss_partial);
+    k_mlp_grad<<<rows / kMlpWarps, kMlpThreads, 0, s>>>(packed, feat, target, idx, nb, 1.f / (float)nb,
+                                                         over_weight, partial, loss_partial);
+}
+
+void launch_mlp_grad_blocks(const MlpPacked* packed, const float* feat, const float* target, int nb, int blocks,
+                            float* partial, float* loss_partial, cudaStream_t s)
+{
+    k_mlp_grad<<<blocks, kMlpThreads, 0, s>>>(packed, feat, target, nullptr, nb, 1.f / (float)nb, 1.f, partial,
+                                               loss_partial);
 }
 
 void launch_mlp_adam(const float* partial, const float* loss_partial, int rows, float* master, float* m1, float* m2,

@@ -249,6 +249,9 @@ class SPHSolver:
     def mlp_record(self, on: bool = True):
         self._call("lsp_mlp_record", 1 if on else 0)
 
+    def mlp_set_loss_asymmetry(self, over_weight: float):
+        self._call("lsp_mlp_set_loss_asymmetry", c_float(over_weight))
+
     def mlp_train(self, iterations: int = 4, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> float:
         """Adam steps on the last recorded step (features -> final pressure); returns the loss."""
         loss = c_float()
