@@ -220,28 +220,38 @@ __device__ __forceinline__ void collide_all(const Collider* cols, int ncoll, V3&
     for (int c = 0; c < ncoll; c++) collide(cols[c], pos, vel, P);
 }
 
-// Walks particle i's neighbour list (column-major, `stride` apart) in list order. Loads of
-// the next B indices are issued together, then the B neighbour records, and only then the
-// per-pair arithmetic f(j, record) runs, in list order: the dependent index -> record
-// loads of B pairs are in flight at once instead of one pair at a time, and every sum
-// still accumulates in the reference's order.
+// Walks particle i's neighbour list (column-major, `stride` apart) in list order, software
+// pipelined: while batch b's records are fetched and its pairs computed, the indices of
+// batch b+1 are already in flight, so the list's DRAM latency overlaps the arithmetic.
+// f(j, record) runs strictly in list order, so every sum accumulates in the reference's
+// order.
 template <int B, typename Load, typename F>
 __device__ __forceinline__ void for_each_neighbor(const int32_t* __restrict__ list, int64_t stride, int cnt,
                                                   Load load, F f)
 {
-    int e = 0;
-    for (; e + B <= cnt; e += B) {
-        int j[B];
+    const int full = cnt / B;
+    int j[B];
+    if (full > 0) {
 #pragma unroll
         for (int u = 0; u < B; u++) j[u] = __ldg(list + u * stride);
         list += B * stride;
+    }
+    for (int b = 0; b < full; b++) {
         decltype(load(0)) r[B];
 #pragma unroll
         for (int u = 0; u < B; u++) r[u] = load(j[u]);
+        int jn[B];
+        if (b + 1 < full) {
+#pragma unroll
+            for (int u = 0; u < B; u++) jn[u] = __ldg(list + u * stride);
+            list += B * stride;
+        }
 #pragma unroll
         for (int u = 0; u < B; u++) f(j[u], r[u]);
+#pragma unroll
+        for (int u = 0; u < B; u++) j[u] = jn[u];
     }
-    for (; e < cnt; e++) {
+    for (int e = full * B; e < cnt; e++) {
         int jj = __ldg(list);
         list += stride;
         f(jj, load(jj));
