@@ -203,6 +203,18 @@ int lsp_mlp_gradient(lsp_solver* s, const float* features, const float* targets,
 /* Features of the last recorded step, caller order, float[8n]. */
 int lsp_read_features(lsp_solver* s, float* out, int64_t n);
 
+/* Allocation-free variant of lsp_mlp_gradient for callers that may not allocate device
+ * memory while they run: every pointer is caller-owned DEVICE memory (features float[8n],
+ * targets float[n], grad float[LSP_MLP_PARAMS], loss float[1], the mean 0.5 r^2), and the
+ * per-warp partial sums use a fixed scratch array inside the library (2.7 MiB on each
+ * device that loads it, kept until the process exits). n <= 16777216 (LSP_ERR_CAPACITY
+ * beyond). Work is queued on the solver's stream; synchronise before reading the outputs.
+ * The first call on a device looks up the scratch address and should come before any
+ * stream capture. Calls that overlap on the GPU share the scratch and race.
+ * No counterpart in the reference. */
+int lsp_mlp_gradient_static(lsp_solver* s, const float* features, const float* targets, int64_t n,
+                            float* grad, float* loss);
+
 /* ---- measurement ---- */
 /* CUDA events on the solver's stream: mark records event `slot` (0..15); elapsed waits for
  * slot_b and returns the device time between the two marks in milliseconds. */
