@@ -1,0 +1,215 @@
+// Per-particle operations of the step, shared by the single-scene kernels (sph.cu,
+// pcisph.cu) and the batched kernels (batch.cu): each function computes one particle's
+// result exactly as the reference CPU solver does (citations at each function), so both
+// kernel families produce the same bits.
+#pragma once
+
+#include "lsp_device.cuh"
+#include "lsp_kernels.h"
+
+namespace lsp {
+
+enum { T_W = 0, T_DW = 1, T_D2W = 2, T_SPIKY_DW = 3, T_VISC_D2W = 4, T_THRESH = 5 };
+
+// Copies table t (the threshold table has one entry more) into shared memory.
+__device__ __forceinline__ void stage_table(float* sm, const float* g, int t)
+{
+    const int len = t == T_THRESH ? kTableSize + 1 : kTableSize;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[t * kTableSize + i];
+}
+
+// SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
+__device__ __forceinline__ void density_one(const DevParams& P, const StepBuffers& b, const float* W, const float* TH,
+                                            int i)
+{
+    const V3 xi = v3(b.pos[i]);
+    float sum = 0.f;
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return b.pos[j]; },
+                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+    float rho = P.mass * sum;
+    float pr = P.stiffness * (rho - P.rho0);
+    if (pr < 0.f) pr *= P.neg;
+    b.rho[i] = rho;
+    b.pres[i] = pr;
+}
+
+// SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248). The
+// reference walks the list up to three times (normal, colour Laplacian when the normal
+// exceeds the threshold, viscosity); each sum is independent, so one walk computes all
+// three with the same per-sum rounding. kGrad adds |grad rho|, a warm-start feature.
+template <bool kGrad>
+__device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float* DW,
+                                                const float* D2W, const float* VD2W, const float* TH, int i)
+{
+    const V3 xi = v3(b.pos[i]);
+    const V3 vi = v3(b.vel[i]);
+    const float rhoi = b.rho[i];
+    V3 F = v3(0.f, 0.f, 0.f);
+    F += v3(P.gx, P.gy, P.gz) * rhoi;
+    V3 normal = v3(0.f, 0.f, 0.f);
+    V3 visc = v3(0.f, 0.f, 0.f);
+    float lap = 0.f;
+    V3 grad = v3(0.f, 0.f, 0.f);   // sum (rho_j - rho_i) / rho_j grad W_ij: a warm-start feature only
+    struct Rec {
+        float4 x, v;
+        float rho;
+    };
+    for_each_neighbor<2>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return Rec{b.pos[j], b.vel[j], b.rho[j]}; },
+                         [&](int j, const Rec& r) {
+                             const V3 xj = v3(r.x);
+                             V3 dir = xi - xj;
+                             float d = mag(xj - xi);
+                             normal += dir * lookup(DW, TH, d, P) / r.rho;
+                             lap += lookup(D2W, TH, d, P) / r.rho;
+                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * lookup(VD2W, TH, d, P);
+                             if (kGrad) grad += dir * (lookup(DW, TH, d, P) * ((r.rho - rhoi) / r.rho));
+                         });
+    if (kGrad) b.gradrho[i] = P.mass * mag(grad);
+    normal *= P.mass;
+    float len = mag(normal);
+    if (len > P.sigma_thr) F += (normal / len) * (-P.sigma * lap * P.mass);
+    visc *= P.viscosity * P.mass;
+    F += visc;
+    b.force[i] = f4(F, 0.f);
+}
+
+// SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
+__device__ __forceinline__ void sph_pressure_one(const DevParams& P, const StepBuffers& b, const float* SDW,
+                                                 const float* TH, int i)
+{
+    const V3 xi = v3(b.pos[i]);
+    const float rhoi = b.rho[i];
+    const float tf = b.pres[i] / (rhoi * rhoi);
+    V3 pf = v3(0.f, 0.f, 0.f);
+    struct Rec {
+        float4 x;
+        float rho, p;
+    };
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return Rec{b.pos[j], b.rho[j], b.pres[j]}; },
+                         [&](int j, const Rec& r) {
+                             if (j == i) return;
+                             const V3 xj = v3(r.x);
+                             float d = mag(xi - xj);
+                             V3 dir = (xi - xj) / d;
+                             pf += dir * lookup(SDW, TH, d, P) * (tf + r.p / (r.rho * r.rho));
+                         });
+    pf *= -(P.mass * rhoi);
+    V3 F = v3(b.force[i]);
+    F += pf;
+    b.force[i] = f4(F, 0.f);
+}
+
+// SPHParticle::integrate (SPHParticle.cpp:30-44) then SPHSolver::handleCollisions
+// (SPHSolver.cpp:337-355) for one particle. With add_pforce the PCISPH pressure force is
+// added first (PCISPHSolver.cpp:166-169).
+__device__ __forceinline__ void integrate_one(const DevParams& P, const StepBuffers& b, int i, int add_pforce)
+{
+    float4 p4 = b.pos[i], v4 = b.vel[i], h4 = b.half[i], o4 = b.old[i];
+    V3 F = v3(b.force[i]);
+    if (add_pforce) F += v3(b.pforce[i]);
+    const float rho = b.rho[i];
+    V3 acc = F / rho;
+    V3 half = v3(h4);
+    float first = v4.w;
+    if (first != 0.f) {
+        half = v3(v4) - acc * P.dt / 2.f;
+        first = 0.f;
+    }
+    V3 old = half;
+    half = v3(half.x + acc.x * P.dt, half.y + acc.y * P.dt, half.z + acc.z * P.dt);
+    V3 x = v3(p4);
+    x = v3(x.x + half.x * P.dt, x.y + half.y * P.dt, x.z + half.z * P.dt);
+    collide_all(b.colliders, P.ncoll, x, half, P);
+    V3 v = (old + half) / 2.f;
+    b.pos[i] = f4(x, p4.w);
+    b.vel[i] = f4(v, first);
+    b.half[i] = f4(half, h4.w);
+    b.old[i] = f4(old, o4.w);
+    if (b.hist) {
+        // Warm-start pressure history: (p_n, p_{n-1}, p_{n-2}) for the next step's features.
+        float4 hs = b.hist[i];
+        b.hist[i] = make_float4(b.pres[i], hs.x, hs.y, 0.f);
+    }
+}
+
+// PCISPHSolver.cpp:67-97 for one particle. Iteration 0 starts from p = 0, F_p = 0
+// (:58-62). aproximateVelocity (:96, SPHParticle.cpp:46-49) sets v = (v_half_old + v_half)/2;
+// within a step it is idempotent, so it is applied in iteration 0 only, after the
+// prediction has read v.
+__device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBuffers& b, int i, int iteration,
+                                                float4* ppos)
+{
+    float4 v4 = b.vel[i];
+    V3 F = v3(b.force[i]);
+    V3 Fp = iteration == 0 ? v3(0.f, 0.f, 0.f) : v3(b.pforce[i]);
+    const float rho = b.rho[i];
+    V3 hv = v3(b.half[i]);
+    V3 acc = (F + Fp) / rho;
+    if (v4.w != 0.f) hv = v3(v4) - acc * P.dt / 2.f;
+    V3 ph = hv + acc * P.dt;
+    V3 px = v3(b.pos[i]) + ph * P.dt;
+    collide_all(b.colliders, P.ncoll, px, ph, P);
+    ppos[i] = f4(px, 0.f);
+    b.phalf[i] = f4(ph, 0.f);
+    if (iteration == 0 && !P.keep_initial_velocity) {
+        V3 v = (v3(b.old[i]) + v3(b.half[i])) / 2.f;
+        b.vel[i] = f4(v, v4.w);
+    }
+}
+
+// PCISPHSolver.cpp:100-126 for one particle; returns |error| (0 for NaN, which the
+// reference's std::max ignores).
+__device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W,
+                                                 const float* TH, int i, int iteration, float4* ppos)
+{
+    const V3 xi = v3(ppos[i]);
+    float sum = 0.f;
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return ppos[j]; },
+                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+    float pd = P.mass * sum;
+    float er = pd - P.rho0;
+    float pp = P.delta * er;
+    if (pp < 0.f) {
+        er *= P.neg;
+        pp *= P.neg;
+    }
+    float p = (iteration == 0 ? 0.f : b.pres[i]) + pp;
+    b.prho[i] = pd;
+    b.err[i] = er;
+    b.pres[i] = p;
+    // p / rho*^2, the per-particle factor of the pressure force, rides in x*.w so the force
+    // pass fetches a neighbour's position and factor in one 16-byte load. Other threads
+    // read only x*.xyz of this element during this pass.
+    reinterpret_cast<float*>(ppos + i)[3] = p / (pd * pd);
+    float a = fabsf(er);
+    return a == a ? a : 0.f;
+}
+
+// PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
+// reference recomputes per pair; the prefactor uses the current density rho_i.
+__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
+                                              const float* TH, int i, const float4* ppos)
+{
+    const float4 pi4 = ppos[i];
+    const V3 xi = v3(pi4);
+    const float tf = pi4.w;
+    V3 pf = v3(0.f, 0.f, 0.f);
+    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+                         [&](int j) { return ppos[j]; },
+                         [&](int j, float4 pj4) {
+                             if (j == i) return;
+                             const V3 xj = v3(pj4);
+                             float d = mag(xj - xi);
+                             V3 dir = (xi - xj) / d;
+                             pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
+                         });
+    pf *= -(P.mass * b.rho[i]);
+    if (isnan(pf.x)) pf = v3(0.f, 0.f, 0.f);
+    b.pforce[i] = f4(pf, 0.f);
+}
+
+}  // namespace lsp

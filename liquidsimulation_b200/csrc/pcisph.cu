@@ -7,6 +7,7 @@
 #include "lsp_device.cuh"
 #include "lsp_kernels.h"
 #include "mlp.cuh"
+#include "particle_ops.cuh"
 
 #include <algorithm>
 
@@ -14,36 +15,9 @@ namespace lsp {
 
 constexpr int kThreads = 256;
 
-enum { T_W = 0, T_SPIKY_DW = 3, T_THRESH = 5 };
-
 __device__ __forceinline__ void stage_thresholds(float* sm, const float* g)
 {
     for (int t = threadIdx.x; t < kTableSize + 1; t += blockDim.x) sm[t] = g[T_THRESH * kTableSize + t];
-}
-
-// PCISPHSolver.cpp:67-97 for one particle. Iteration 0 starts from p = 0, F_p = 0
-// (:58-62). aproximateVelocity (:96, SPHParticle.cpp:46-49) sets v = (v_half_old + v_half)/2;
-// within a step it is idempotent, so it is applied in iteration 0 only, after the
-// prediction has read v.
-__device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBuffers& b, int i, int iteration,
-                                                float4* ppos)
-{
-    float4 v4 = b.vel[i];
-    V3 F = v3(b.force[i]);
-    V3 Fp = iteration == 0 ? v3(0.f, 0.f, 0.f) : v3(b.pforce[i]);
-    const float rho = b.rho[i];
-    V3 hv = v3(b.half[i]);
-    V3 acc = (F + Fp) / rho;
-    if (v4.w != 0.f) hv = v3(v4) - acc * P.dt / 2.f;
-    V3 ph = hv + acc * P.dt;
-    V3 px = v3(b.pos[i]) + ph * P.dt;
-    collide_all(b.colliders, P.ncoll, px, ph, P);
-    ppos[i] = f4(px, 0.f);
-    b.phalf[i] = f4(ph, 0.f);
-    if (iteration == 0 && !P.keep_initial_velocity) {
-        V3 v = (v3(b.old[i]) + v3(b.half[i])) / 2.f;
-        b.vel[i] = f4(v, v4.w);
-    }
 }
 
 __global__ void __launch_bounds__(kThreads) k_pci_predict(DevParams P, StepBuffers b, int iteration)
@@ -52,35 +26,6 @@ __global__ void __launch_bounds__(kThreads) k_pci_predict(DevParams P, StepBuffe
     if (i == 0) b.status->max_err_bits = 0u;
     if (i >= P.n) return;
     pci_predict_one(P, b, i, iteration, b.ppos);
-}
-
-// PCISPHSolver.cpp:100-126 for one particle; returns |error| (0 for NaN, which the
-// reference's std::max ignores).
-__device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W,
-                                                 const float* TH, int i, int iteration, float4* ppos)
-{
-    const V3 xi = v3(ppos[i]);
-    float sum = 0.f;
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
-                         [&](int j) { return ppos[j]; },
-                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
-    float pd = P.mass * sum;
-    float er = pd - P.rho0;
-    float pp = P.delta * er;
-    if (pp < 0.f) {
-        er *= P.neg;
-        pp *= P.neg;
-    }
-    float p = (iteration == 0 ? 0.f : b.pres[i]) + pp;
-    b.prho[i] = pd;
-    b.err[i] = er;
-    b.pres[i] = p;
-    // p / rho*^2, the per-particle factor of the pressure force, rides in x*.w so the force
-    // pass fetches a neighbour's position and factor in one 16-byte load. Other threads
-    // read only x*.xyz of this element during this pass.
-    reinterpret_cast<float*>(ppos + i)[3] = p / (pd * pd);
-    float a = fabsf(er);
-    return a == a ? a : 0.f;
 }
 
 __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffers b, int iteration)
@@ -103,29 +48,6 @@ __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffe
         for (int w = 0; w < kThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
         if (bm) atomicMax(&b.status->max_err_bits, bm);
     }
-}
-
-// PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
-// reference recomputes per pair; the prefactor uses the current density rho_i.
-__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
-                                              const float* TH, int i, const float4* ppos)
-{
-    const float4 pi4 = ppos[i];
-    const V3 xi = v3(pi4);
-    const float tf = pi4.w;
-    V3 pf = v3(0.f, 0.f, 0.f);
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
-                         [&](int j) { return ppos[j]; },
-                         [&](int j, float4 pj4) {
-                             if (j == i) return;
-                             const V3 xj = v3(pj4);
-                             float d = mag(xj - xi);
-                             V3 dir = (xi - xj) / d;
-                             pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
-                         });
-    pf *= -(P.mass * b.rho[i]);
-    if (isnan(pf.x)) pf = v3(0.f, 0.f, 0.f);
-    b.pforce[i] = f4(pf, 0.f);
 }
 
 __global__ void __launch_bounds__(kThreads) k_pci_force(DevParams P, StepBuffers b)
