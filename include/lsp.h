@@ -242,6 +242,79 @@ int lsp_launch_count(const lsp_solver* s, int64_t* launches);
 int lsp_host_alloc(size_t bytes, void** out);
 int lsp_host_free(void* p);
 
+/*
+ * ---- batches of independent scenes ----
+ *
+ * A batch steps many scenes together on one device: what the reference does with one
+ * SPHSolver / PCISPHSolver object per scene, each updated in turn by its
+ * PhysicSolver::update (PhysicSolver.cpp:12-21). Each scene keeps its own parameters,
+ * particles (caller order within the scene), colliders and grid, and its results are
+ * bit-identical to a single-scene handle given the same inputs. All scenes of a batch use
+ * the same solver kind and step with the same dt. The whole step of all scenes runs as one
+ * CUDA graph with one persistent kernel for the PCISPH loops of all scenes, each scene
+ * converging on its own. Scenes and colliders are added before the first step; colliders
+ * can be moved at any time. No counterpart in the reference (it has no batching).
+ */
+typedef struct lsp_batch lsp_batch;
+
+typedef struct lsp_batch_tuning {
+    int32_t threads;        /* chosen particles per block of the per-particle kernels */
+    int32_t loop_blocks;    /* chosen blocks of the persistent PCISPH kernel */
+    int32_t candidates;     /* configurations timed (<= 16) */
+    int32_t reserved;
+    int32_t cand_threads[16];
+    int32_t cand_loop_blocks[16];
+    float cand_ms[16];      /* best device time of one step, per configuration */
+} lsp_batch_tuning;
+
+/* device < 0: the current device. */
+int lsp_batch_create(int device, lsp_batch** out);
+int lsp_batch_destroy(lsp_batch* b);
+/* Adds a scene: n >= 1 particles in caller order (vel may be NULL = zero). domain_lo/hi
+ * (both or neither) fix the grid box like lsp_set_domain; without them it is the union of
+ * the scene's boundary colliders at its first step, else the particle bounds plus a margin.
+ * Writes the scene index (0, 1, ...). */
+int lsp_batch_add_scene(lsp_batch* b, const lsp_params* params, const float* xyz, const float* vel, int64_t n,
+                        const float* domain_lo, const float* domain_hi, int32_t* scene);
+int lsp_batch_add_box(lsp_batch* b, int32_t scene, const float center[3], const float half_extent[3], int kind);
+int lsp_batch_add_sphere(lsp_batch* b, int32_t scene, const float center[3], float radius, int kind);
+/* Moves collider `index` of a scene (its kind and shape stay). */
+int lsp_batch_update_box(lsp_batch* b, int32_t scene, int32_t index, const float center[3],
+                         const float half_extent[3]);
+int lsp_batch_update_sphere(lsp_batch* b, int32_t scene, int32_t index, const float center[3], float radius);
+int lsp_batch_info(const lsp_batch* b, int32_t* scenes, int64_t* particles);
+int lsp_batch_scene_count(const lsp_batch* b, int32_t scene, int64_t* n);
+int lsp_batch_particle_mass(const lsp_batch* b, int32_t scene, float* mass);
+/* One step of every scene. stats: NULL or an array of one lsp_step_stats per scene. */
+int lsp_batch_step(lsp_batch* b, float dt, lsp_step_stats* stats);
+/* Per-scene read-back in the scene's caller order (n = the scene's particle count). */
+int lsp_batch_read_particles(lsp_batch* b, int32_t scene, float* xyz, float* vel, int64_t n);
+int lsp_batch_read_field(lsp_batch* b, int32_t scene, int field, float* out, int64_t n);
+int lsp_batch_read_neighbors(lsp_batch* b, int32_t scene, int64_t* offsets, int32_t* index, int64_t n,
+                             int64_t capacity);
+int lsp_batch_grid_info(const lsp_batch* b, int32_t scene, int32_t dims[3], int32_t origin[3], int64_t* cells);
+int lsp_batch_read_grid(lsp_batch* b, int32_t scene, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start,
+                        int64_t cells_plus_one);
+/* The whole batch's state, scenes concatenated in index order, each in caller order
+ * (n = total particles; same arrays as lsp_read_state / lsp_write_state). */
+int lsp_batch_read_state(lsp_batch* b, float* x, float* v, float* v_half, float* v_half_old, int32_t* first_step,
+                         int64_t n);
+int lsp_batch_write_state(lsp_batch* b, const float* x, const float* v, const float* v_half,
+                          const float* v_half_old, const int32_t* first_step, int64_t n);
+/* Launch shape: use_graph (0/1), threads (128, 256 or 512 particles per block), loop_blocks
+ * (blocks of the persistent kernel, 0 = all that fit). get also reports whether the step
+ * currently runs as a captured graph. */
+int lsp_batch_set_launch(lsp_batch* b, int use_graph, int threads, int loop_blocks);
+int lsp_batch_get_launch(const lsp_batch* b, int* use_graph, int* threads, int* loop_blocks, int* graph_active);
+/* Autotuner: runs the next step under each candidate launch shape (particles per block x
+ * persistent-kernel blocks), re-running that same step from the same state `repeats` times
+ * per candidate, keeps the fastest shape, and leaves the batch advanced by exactly that one
+ * step (results do not depend on the shape). result and stats may be NULL. */
+int lsp_batch_autotune(lsp_batch* b, float dt, int repeats, lsp_batch_tuning* result, lsp_step_stats* stats);
+int lsp_batch_timer_mark(lsp_batch* b, int slot);
+int lsp_batch_timer_elapsed(lsp_batch* b, int slot_a, int slot_b, float* ms);
+int lsp_batch_launch_count(const lsp_batch* b, int64_t* launches);
+
 #ifdef __cplusplus
 }
 #endif

@@ -96,6 +96,18 @@ class LspStepStats(ctypes.Structure):
     ]
 
 
+class LspBatchTuning(ctypes.Structure):
+    _fields_ = [
+        ("threads", c_int32),
+        ("loop_blocks", c_int32),
+        ("candidates", c_int32),
+        ("reserved", c_int32),
+        ("cand_threads", c_int32 * 16),
+        ("cand_loop_blocks", c_int32 * 16),
+        ("cand_ms", c_float * 16),
+    ]
+
+
 def default_params(**overrides) -> LspParams:
     """The reference's constructor defaults, then ``overrides`` by field name."""
     p = LspParams()
@@ -220,6 +232,31 @@ def _declare(lib):
         "lsp_mlp_forward": (c_int, [S, fp, c_int64, fp]),
         "lsp_mlp_gradient": (c_int, [S, fp, fp, c_int64, fp, fp]),
         "lsp_read_features": (c_int, [S, fp, c_int64]),
+        # batches of independent scenes
+        "lsp_batch_create": (c_int, [c_int, POINTER(c_void_p)]),
+        "lsp_batch_destroy": (c_int, [c_void_p]),
+        "lsp_batch_add_scene": (c_int, [c_void_p, POINTER(LspParams), fp, fp, c_int64, fp, fp, i32p]),
+        "lsp_batch_add_box": (c_int, [c_void_p, c_int32, fp, fp, c_int]),
+        "lsp_batch_add_sphere": (c_int, [c_void_p, c_int32, fp, c_float, c_int]),
+        "lsp_batch_update_box": (c_int, [c_void_p, c_int32, c_int32, fp, fp]),
+        "lsp_batch_update_sphere": (c_int, [c_void_p, c_int32, c_int32, fp, c_float]),
+        "lsp_batch_info": (c_int, [c_void_p, i32p, i64p]),
+        "lsp_batch_scene_count": (c_int, [c_void_p, c_int32, i64p]),
+        "lsp_batch_particle_mass": (c_int, [c_void_p, c_int32, fp]),
+        "lsp_batch_step": (c_int, [c_void_p, c_float, POINTER(LspStepStats)]),
+        "lsp_batch_read_particles": (c_int, [c_void_p, c_int32, fp, fp, c_int64]),
+        "lsp_batch_read_field": (c_int, [c_void_p, c_int32, c_int, fp, c_int64]),
+        "lsp_batch_read_neighbors": (c_int, [c_void_p, c_int32, i64p, i32p, c_int64, c_int64]),
+        "lsp_batch_grid_info": (c_int, [c_void_p, c_int32, i32p, i32p, i64p]),
+        "lsp_batch_read_grid": (c_int, [c_void_p, c_int32, u32p, i32p, c_int64, u32p, c_int64]),
+        "lsp_batch_read_state": (c_int, [c_void_p, fp, fp, fp, fp, i32p, c_int64]),
+        "lsp_batch_write_state": (c_int, [c_void_p, fp, fp, fp, fp, i32p, c_int64]),
+        "lsp_batch_set_launch": (c_int, [c_void_p, c_int, c_int, c_int]),
+        "lsp_batch_get_launch": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+        "lsp_batch_autotune": (c_int, [c_void_p, c_float, c_int, POINTER(LspBatchTuning), POINTER(LspStepStats)]),
+        "lsp_batch_timer_mark": (c_int, [c_void_p, c_int]),
+        "lsp_batch_timer_elapsed": (c_int, [c_void_p, c_int, c_int, fp]),
+        "lsp_batch_launch_count": (c_int, [c_void_p, i64p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -10,12 +10,7 @@
 
 namespace lsp {
 
-#define CK(call)                                                                                  \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            throw Error(LSP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
-    } while (0)
+#define CK(call) LSP_CK(call)
 
 // ------------------------------------------------------------------ host kernels
 // SPHKernel::setRadius / recalcCachedWeights (SPHKernel.cpp:93-137) with the poly6,
@@ -111,32 +106,8 @@ float HostKernels::delta(const lsp_params& p, float dt) const
     return delta;
 }
 
-// ------------------------------------------------------------------ device arrays
-template <typename T>
-void DevArray<T>::alloc(size_t count)
-{
-    release();
-    if (count == 0) return;
-    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
-    if (e != cudaSuccess) {
-        p = nullptr;
-        throw Error(e == cudaErrorMemoryAllocation ? LSP_ERR_CAPACITY : LSP_ERR_CUDA,
-                    std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
-                        cudaGetErrorString(e));
-    }
-    n = count;
-}
-
-template <typename T>
-void DevArray<T>::release()
-{
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-}
-
 // ------------------------------------------------------------------ engine
-static void validate(const lsp_params& p)
+void validate_params(const lsp_params& p)
 {
     auto bad = [](const char* m) { throw Error(LSP_ERR_INVALID, m); };
     if (!(p.particle_radius > 0.f) || !std::isfinite(p.particle_radius)) bad("particle_radius must be > 0");
@@ -151,7 +122,7 @@ static void validate(const lsp_params& p)
 
 Engine::Engine(const lsp_params& p, int device)
 {
-    validate(p);
+    validate_params(p);
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) throw Error(LSP_ERR_NO_DEVICE, "no CUDA device");
     if (device < 0) CK(cudaGetDevice(&device));
@@ -196,7 +167,7 @@ void Engine::derive()
 
 void Engine::set_params(const lsp_params& p)
 {
-    validate(p);
+    validate_params(p);
     bool geometry = p.particle_radius != prm_.particle_radius || p.kernel_radius_factor != prm_.kernel_radius_factor;
     prm_ = p;
     derive();
@@ -359,18 +330,7 @@ void Engine::ensure_grid()
         std::memcpy(hi, dom_hi_, sizeof(hi));
         have = true;
     } else {
-        for (const Collider& c : cols_) {
-            if (!c.boundary) continue;
-            float cc[3] = {c.cx, c.cy, c.cz};
-            float e[3] = {c.hx, c.hy, c.hz};
-            if (c.sphere) e[0] = e[1] = e[2] = c.radius;
-            for (int a = 0; a < 3; a++) {
-                float l = cc[a] - std::fabs(e[a]), u = cc[a] + std::fabs(e[a]);
-                lo[a] = have ? std::min(lo[a], l) : l;
-                hi[a] = have ? std::max(hi[a], u) : u;
-            }
-            have = true;
-        }
+        have = boundary_box(cols_, lo, hi);
     }
     if (!have && n_ > 0) {
         activate();
@@ -394,14 +354,7 @@ void Engine::ensure_grid()
         }
         domain_from_particles_ = true;
     }
-    int64_t cells = 1;
-    for (int a = 0; a < 3; a++) {
-        int c0 = (int)(lo[a] / hk_.h), c1 = (int)(hi[a] / hk_.h);
-        org_[a] = c0;
-        dim_[a] = std::max(1, c1 - c0 + 1);
-        cells *= dim_[a];
-    }
-    if (cells > ((int64_t)1 << 30)) throw Error(LSP_ERR_CAPACITY, "grid box holds more than 2^30 cells of size h");
+    const int64_t cells = grid_from_box(lo, hi, hk_.h, org_, dim_);
     cells_ = cells;
     if (cells + 1 > cells_alloc_) {
         activate();
@@ -416,37 +369,74 @@ void Engine::ensure_grid()
     grid_valid_ = true;
 }
 
-DevParams Engine::device_params(float dt) const
+bool boundary_box(const std::vector<Collider>& cols, float lo[3], float hi[3])
+{
+    bool have = false;
+    for (const Collider& c : cols) {
+        if (!c.boundary) continue;
+        float cc[3] = {c.cx, c.cy, c.cz};
+        float e[3] = {c.hx, c.hy, c.hz};
+        if (c.sphere) e[0] = e[1] = e[2] = c.radius;
+        for (int a = 0; a < 3; a++) {
+            float l = cc[a] - std::fabs(e[a]), u = cc[a] + std::fabs(e[a]);
+            lo[a] = have ? std::min(lo[a], l) : l;
+            hi[a] = have ? std::max(hi[a], u) : u;
+        }
+        have = true;
+    }
+    return have;
+}
+
+int64_t grid_from_box(const float lo[3], const float hi[3], float h, int32_t org[3], int32_t dim[3])
+{
+    int64_t cells = 1;
+    for (int a = 0; a < 3; a++) {
+        int c0 = (int)(lo[a] / h), c1 = (int)(hi[a] / h);
+        org[a] = c0;
+        dim[a] = std::max(1, c1 - c0 + 1);
+        cells *= dim[a];
+    }
+    if (cells > ((int64_t)1 << 30)) throw Error(LSP_ERR_CAPACITY, "grid box holds more than 2^30 cells of size h");
+    return cells;
+}
+
+DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt)
 {
     DevParams P{};
-    P.gx = prm_.gravity[0]; P.gy = prm_.gravity[1]; P.gz = prm_.gravity[2];
-    P.h = hk_.h;
-    P.h2 = hk_.h * hk_.h;
-    P.step = hk_.step;
-    P.inv_step = 1.f / hk_.step;
-    P.radius = prm_.particle_radius;
-    P.mass = hk_.mass;
-    P.rho0 = prm_.rest_density;
-    P.stiffness = prm_.stiffness;
-    P.neg = prm_.negative_pressure_factor;
-    P.viscosity = prm_.viscosity;
-    P.sigma = prm_.surface_tension;
-    P.sigma_thr = prm_.surface_tension_threshold;
-    P.restitution = prm_.restitution;
-    P.friction = prm_.friction;
-    P.delta = prm_.solver == LSP_SOLVER_PCISPH ? hk_.delta(prm_, dt) : 0.f;
-    P.eta = prm_.pci_eta;
+    P.gx = p.gravity[0]; P.gy = p.gravity[1]; P.gz = p.gravity[2];
+    P.h = hk.h;
+    P.h2 = hk.h * hk.h;
+    P.step = hk.step;
+    P.inv_step = 1.f / hk.step;
+    P.radius = p.particle_radius;
+    P.mass = hk.mass;
+    P.rho0 = p.rest_density;
+    P.stiffness = p.stiffness;
+    P.neg = p.negative_pressure_factor;
+    P.viscosity = p.viscosity;
+    P.sigma = p.surface_tension;
+    P.sigma_thr = p.surface_tension_threshold;
+    P.restitution = p.restitution;
+    P.friction = p.friction;
+    P.delta = p.solver == LSP_SOLVER_PCISPH ? hk.delta(p, dt) : 0.f;
+    P.eta = p.pci_eta;
     P.dt = dt;
+    P.keep_initial_velocity = p.keep_initial_velocity;
+    P.min_it = p.pci_min_iterations;
+    P.max_it = p.pci_max_iterations;
+    return P;
+}
+
+DevParams Engine::device_params(float dt) const
+{
+    DevParams P = physics_params(prm_, hk_, dt);
     P.n = (int)n_;
-    P.keep_initial_velocity = prm_.keep_initial_velocity;
     P.ncoll = (int)cols_.size();
     P.ox = org_[0]; P.oy = org_[1]; P.oz = org_[2];
     P.nx = dim_[0]; P.ny = dim_[1]; P.nz = dim_[2];
     P.cells = (uint32_t)cells_;
     P.nbr_cap = nbr_cap_;
     P.nbr_stride = nbr_stride_;
-    P.min_it = prm_.pci_min_iterations;
-    P.max_it = prm_.pci_max_iterations;
     return P;
 }
 
@@ -632,7 +622,7 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
     return false;
 }
 
-static int initial_neighbor_capacity(const lsp_params& p)
+int initial_neighbor_capacity(const lsp_params& p)
 {
     // Lattice estimate (4/3) pi (h/s)^3 with s = 1.6 r, doubled for compression.
     double q = p.kernel_radius_factor / 1.6;

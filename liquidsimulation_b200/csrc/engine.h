@@ -32,10 +32,50 @@ template <typename T>
 struct DevArray {
     T* p = nullptr;
     size_t n = 0;
-    void alloc(size_t count);
-    void release();
+    void alloc(size_t count)
+    {
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw Error(e == cudaErrorMemoryAllocation ? LSP_ERR_CAPACITY : LSP_ERR_CUDA,
+                        std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
+                            cudaGetErrorString(e));
+        }
+        n = count;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    DevArray() = default;
+    DevArray(const DevArray&) = delete;
+    DevArray& operator=(const DevArray&) = delete;
     ~DevArray() { release(); }
 };
+
+#define LSP_CK(call)                                                                              \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            throw ::lsp::Error(LSP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Parameter checks shared by single scenes and batches (LSP_ERR_INVALID on failure).
+void validate_params(const lsp_params& p);
+// Union of the boundary colliders' boxes; false when there is none.
+bool boundary_box(const std::vector<Collider>& cols, float lo[3], float hi[3]);
+// Grid origin and dimensions (cells of size h, c = (int)(x / h)) covering [lo, hi]; returns
+// the cell count (LSP_ERR_CAPACITY above 2^30).
+int64_t grid_from_box(const float lo[3], const float hi[3], float h, int32_t org[3], int32_t dim[3]);
+// DevParams fields that follow from the parameters, the derived kernel constants and dt
+// (everything except the particle count, grid, colliders and neighbour-list layout).
+DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt);
+// First neighbour-list capacity: twice the lattice estimate of the neighbour count.
+int initial_neighbor_capacity(const lsp_params& p);
 
 class Engine {
 public:

@@ -19,8 +19,8 @@
 //   k_rank_gather deterministic rank by caller id inside each cell, then one gather of
 //                 the 64-byte persistent state into the new order
 //   k_neighbors   the start-of-step neighbour lists, column-major, reference order
-#include "lsp_device.cuh"
 #include "lsp_kernels.h"
+#include "particle_ops.cuh"
 
 namespace lsp {
 
@@ -29,54 +29,20 @@ constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 constexpr int kMaxCellOccupancy = 4096;
 
-__device__ __forceinline__ uint32_t lanemask_lt()
-{
-    uint32_t m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
 __global__ void k_keys_hist(DevParams P, const float4* __restrict__ pos, uint32_t* __restrict__ key,
                             uint32_t* __restrict__ slot, uint32_t* __restrict__ hist, DevStatus* st)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = i < P.n;
-    const int lane = threadIdx.x & 31;
     uint32_t k = 0xffffffffu;
     bool escaped = false, bad = false;
-    if (valid) {
-        float4 p = pos[i];
-        bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
-        int c[3] = {cell_coord(p.x, P.h), cell_coord(p.y, P.h), cell_coord(p.z, P.h)};
-        const int o[3] = {P.ox, P.oy, P.oz};
-        const int d[3] = {P.nx, P.ny, P.nz};
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            int v = c[a];
-            if (v < o[a]) { v = o[a]; escaped = true; }
-            if (v > o[a] + d[a] - 1) { v = o[a] + d[a] - 1; escaped = true; }
-            c[a] = v - o[a];
-        }
-        k = (uint32_t)(((uint32_t)c[0] * (uint32_t)P.ny + (uint32_t)c[1]) * (uint32_t)P.nz + (uint32_t)c[2]);
-    }
-    // Warp-aggregated histogram: one atomic per distinct key in the warp; lanes with the
-    // same key take consecutive slots in lane order.
-    uint32_t peers = __match_any_sync(0xffffffffu, k);
-    uint32_t leader = __ffs(peers) - 1;
-    uint32_t rank = __popc(peers & lanemask_lt());
-    uint32_t base = 0;
-    if (valid && lane == (int)leader) base = atomicAdd(&hist[k], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
+    if (valid) k = cell_key(P, pos[i], escaped, bad);
+    const uint32_t sl = hist_slot(k, valid, hist);
     if (valid) {
         key[i] = k;
-        slot[i] = base + rank;
+        slot[i] = sl;
     }
-    uint32_t esc = __ballot_sync(0xffffffffu, valid && escaped);
-    uint32_t nan = __ballot_sync(0xffffffffu, valid && bad);
-    if (lane == 0) {
-        if (esc) atomicAdd(&st->escaped, (uint32_t)__popc(esc));
-        if (nan) atomicOr(&st->error_flags, kErrNaN);
-    }
+    record_key_flags(valid, escaped, bad, st);
 }
 
 // Block-wide exclusive scan of kScanItems consecutive items per thread, warp shuffles
@@ -208,10 +174,7 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
     sorted_key[dest] = k;
 }
 
-// Start-of-step neighbour list of each particle: every j with |x_i - x_j|^2 <= h^2,
-// including i, in the reference's order (SPHSpatialGrid::findNeighborParticles,
-// SPHSpatialGrid.cpp:39-76): cell ranges from (x -+ h) / h per axis, x then y rows,
-// each row a contiguous z-run of the sorted array.
+// Start-of-step neighbour lists (neighbors_one), column-major.
 __global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ cell_start,
                             int32_t* __restrict__ nbr, int32_t* __restrict__ count, DevStatus* st)
 {
@@ -219,55 +182,36 @@ __global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const u
     const bool valid = i < P.n;
     int c = 0;
     if (valid) {
-        const float4 pi = pos[i];
-        const V3 xi = v3(pi);
-        const float h = P.h;
-        int lo[3] = {(int)((xi.x - h) / h), (int)((xi.y - h) / h), (int)((xi.z - h) / h)};
-        int hi[3] = {(int)((xi.x + h) / h), (int)((xi.y + h) / h), (int)((xi.z + h) / h)};
-        const int o[3] = {P.ox, P.oy, P.oz};
-        const int d[3] = {P.nx, P.ny, P.nz};
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            // Both ends clamped into the box: a particle outside it searches the edge
-            // cell that holds every clamped particle.
-            lo[a] = min(max(lo[a], o[a]), o[a] + d[a] - 1) - o[a];
-            hi[a] = min(max(hi[a], o[a]), o[a] + d[a] - 1) - o[a];
-        }
-        const int cap = P.nbr_cap;
-        const int64_t stride = P.nbr_stride;
-        if (lo[2] <= hi[2]) {
-            for (int cx = lo[0]; cx <= hi[0]; cx++) {
-                for (int cy = lo[1]; cy <= hi[1]; cy++) {
-                    uint32_t row = ((uint32_t)cx * (uint32_t)P.ny + (uint32_t)cy) * (uint32_t)P.nz;
-                    uint32_t beg = cell_start[row + lo[2]];
-                    uint32_t end = cell_start[row + hi[2] + 1];
-                    for (uint32_t q = beg; q < end; q++) {
-                        V3 dq = xi - v3(pos[q]);
-                        if (sqmag(dq) <= P.h2) {
-                            if (c < cap) nbr[(int64_t)c * stride + i] = (int32_t)q;
-                            c++;
-                        }
-                    }
-                }
-            }
-        }
-        // The stored count never exceeds the list capacity, so later passes stay inside the
-        // list even in an overflowed step; the true count only feeds the maximum below.
-        count[i] = min(c, cap);
+        c = neighbors_one(P, pos, cell_start, nbr, i);
+        count[i] = min(c, P.nbr_cap);
     }
-    // Overflow flag and the step's maximum count: one atomic per warp.
-    uint32_t m = (uint32_t)c;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
-    if ((threadIdx.x & 31) == 0 && m > 0) {
-        atomicMax(&st->max_neighbors, m);
-        if (m > (uint32_t)P.nbr_cap) atomicOr(&st->error_flags, kErrNeighborOverflow);
-    }
+    record_neighbor_count(P, c, valid, st);
 }
 
 // ------------------------------------------------------------------ launchers
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+int launch_grid_order(const GridBuildArgs& a, cudaStream_t s)
+{
+    const int T = 256;
+    const DevParams& P = a.P;
+    const int64_t n = (int64_t)P.cells + 1;
+    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
+    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
+    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
+    int launches = 3;
+    if (P.n > 0) {
+        k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
+        k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
+                                                       a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
+                                                       a.old_out, a.slot_of_id, a.sorted_key, a.status, a.hist_in,
+                                                       a.hist_out);
+        launches += 2;
+    }
+    return launches;
+}
 
 int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s)
 {
@@ -278,21 +222,7 @@ int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s)
         k_keys_hist<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.hist, a.status);
         launches++;
     }
-    const int64_t n = (int64_t)P.cells + 1;
-    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
-    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
-    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
-    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
-    launches += 3;
-    if (P.n > 0) {
-        k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
-        k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
-                                                       a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
-                                                       a.old_out, a.slot_of_id, a.sorted_key, a.status, a.hist_in,
-                                                       a.hist_out);
-        launches += 2;
-    }
-    return launches;
+    return launches + launch_grid_order(a, s);
 }
 
 int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)

@@ -77,6 +77,12 @@ struct DevParams {
     int nbr_cap;        // neighbour list capacity per particle
     int64_t nbr_stride; // column stride of the neighbour list (>= n)
     int min_it, max_it;
+    // Batches of scenes (all zero for a single scene): the scene's first particle slot,
+    // its first cell in the batch's cell table and its first collider.
+    int base;
+    uint32_t cell_base;
+    int coll_off;
+    int scene;
 };
 
 // ----------------------------------------------------------------- vector ops

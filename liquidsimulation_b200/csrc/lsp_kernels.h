@@ -71,8 +71,11 @@ struct StepBuffers {
     DevStatus* status;
 };
 
-// Both return the number of kernels launched.
+// All return the number of kernels launched.
 int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
+// The part of the grid build after the keys: scan of a.hist (a.P.cells + 1 counters) into
+// the cell table, scatter, rank by caller id and gather of a.P.n particles.
+int launch_grid_order(const GridBuildArgs& a, cudaStream_t s);
 int launch_neighbors(const GridBuildArgs& a, cudaStream_t s);
 
 void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s);

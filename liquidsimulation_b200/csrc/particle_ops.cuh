@@ -18,6 +18,117 @@ __device__ __forceinline__ void stage_table(float* sm, const float* g, int t)
     for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[t * kTableSize + i];
 }
 
+// Cell key of a position inside the scene's grid box: the CPU grid's cell (int)(x / h)
+// per axis (SPHSpatialGrid.cpp:80-82), clamped into the box, ordered x slowest and z
+// fastest, plus the scene's first cell in a batch.
+__device__ __forceinline__ uint32_t cell_key(const DevParams& P, const float4& p, bool& escaped, bool& bad)
+{
+    bad = !(isfinite(p.x) && isfinite(p.y) && isfinite(p.z));
+    int c[3] = {cell_coord(p.x, P.h), cell_coord(p.y, P.h), cell_coord(p.z, P.h)};
+    const int o[3] = {P.ox, P.oy, P.oz};
+    const int d[3] = {P.nx, P.ny, P.nz};
+    escaped = false;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        int v = c[a];
+        if (v < o[a]) { v = o[a]; escaped = true; }
+        if (v > o[a] + d[a] - 1) { v = o[a] + d[a] - 1; escaped = true; }
+        c[a] = v - o[a];
+    }
+    return P.cell_base + (uint32_t)(((uint32_t)c[0] * (uint32_t)P.ny + (uint32_t)c[1]) * (uint32_t)P.nz + (uint32_t)c[2]);
+}
+
+// Start-of-step neighbour list of particle i: every j with |x_i - x_j|^2 <= h^2,
+// including i, in the reference's order (SPHSpatialGrid::findNeighborParticles,
+// SPHSpatialGrid.cpp:39-76): cell ranges from (x -+ h) / h per axis, x then y rows,
+// each row a contiguous z-run of the sorted array. Stores at most nbr_cap entries and
+// returns the true count.
+__device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* __restrict__ pos,
+                                             const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
+                                             int i)
+{
+    const float4 pi = pos[i];
+    const V3 xi = v3(pi);
+    const float h = P.h;
+    int lo[3] = {(int)((xi.x - h) / h), (int)((xi.y - h) / h), (int)((xi.z - h) / h)};
+    int hi[3] = {(int)((xi.x + h) / h), (int)((xi.y + h) / h), (int)((xi.z + h) / h)};
+    const int o[3] = {P.ox, P.oy, P.oz};
+    const int d[3] = {P.nx, P.ny, P.nz};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        // Both ends clamped into the box: a particle outside it searches the edge cell
+        // that holds every clamped particle.
+        lo[a] = min(max(lo[a], o[a]), o[a] + d[a] - 1) - o[a];
+        hi[a] = min(max(hi[a], o[a]), o[a] + d[a] - 1) - o[a];
+    }
+    const int cap = P.nbr_cap;
+    const int64_t stride = P.nbr_stride;
+    int c = 0;
+    if (lo[2] <= hi[2]) {
+        for (int cx = lo[0]; cx <= hi[0]; cx++) {
+            for (int cy = lo[1]; cy <= hi[1]; cy++) {
+                uint32_t row = P.cell_base + ((uint32_t)cx * (uint32_t)P.ny + (uint32_t)cy) * (uint32_t)P.nz;
+                uint32_t beg = cell_start[row + lo[2]];
+                uint32_t end = cell_start[row + hi[2] + 1];
+                for (uint32_t q = beg; q < end; q++) {
+                    V3 dq = xi - v3(pos[q]);
+                    if (sqmag(dq) <= P.h2) {
+                        if (c < cap) nbr[(int64_t)c * stride + i] = (int32_t)q;
+                        c++;
+                    }
+                }
+            }
+        }
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated histogram of cell keys: one atomic per distinct key in the warp; lanes
+// with the same key take consecutive slots in lane order. All 32 lanes must call it.
+__device__ __forceinline__ uint32_t hist_slot(uint32_t k, bool valid, uint32_t* hist)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t peers = __match_any_sync(0xffffffffu, k);
+    uint32_t leader = __ffs(peers) - 1;
+    uint32_t rank = __popc(peers & lanemask_lt());
+    uint32_t base = 0;
+    if (valid && lane == (int)leader) base = atomicAdd(&hist[k], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return base + rank;
+}
+
+// Escaped and non-finite positions of the warp, one atomic each. All 32 lanes call it.
+__device__ __forceinline__ void record_key_flags(bool valid, bool escaped, bool bad, DevStatus* st)
+{
+    uint32_t esc = __ballot_sync(0xffffffffu, valid && escaped);
+    uint32_t nan = __ballot_sync(0xffffffffu, valid && bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (esc) atomicAdd(&st->escaped, (uint32_t)__popc(esc));
+        if (nan) atomicOr(&st->error_flags, kErrNaN);
+    }
+}
+
+// The stored neighbour count never exceeds the list capacity, so later passes stay inside
+// the list even in an overflowed step; the true count only feeds the step's maximum and the
+// overflow flag (one atomic per warp). All 32 lanes call it.
+__device__ __forceinline__ void record_neighbor_count(const DevParams& P, int c, bool valid, DevStatus* st)
+{
+    uint32_t m = valid ? (uint32_t)c : 0u;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0 && m > 0) {
+        atomicMax(&st->max_neighbors, m);
+        if (m > (uint32_t)P.nbr_cap) atomicOr(&st->error_flags, kErrNeighborOverflow);
+    }
+}
+
 // SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
 __device__ __forceinline__ void density_one(const DevParams& P, const StepBuffers& b, const float* W, const float* TH,
                                             int i)
@@ -122,7 +233,7 @@ __device__ __forceinline__ void integrate_one(const DevParams& P, const StepBuff
     half = v3(half.x + acc.x * P.dt, half.y + acc.y * P.dt, half.z + acc.z * P.dt);
     V3 x = v3(p4);
     x = v3(x.x + half.x * P.dt, x.y + half.y * P.dt, x.z + half.z * P.dt);
-    collide_all(b.colliders, P.ncoll, x, half, P);
+    collide_all(b.colliders + P.coll_off, P.ncoll, x, half, P);
     V3 v = (old + half) / 2.f;
     b.pos[i] = f4(x, p4.w);
     b.vel[i] = f4(v, first);
@@ -151,7 +262,7 @@ __device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBu
     if (v4.w != 0.f) hv = v3(v4) - acc * P.dt / 2.f;
     V3 ph = hv + acc * P.dt;
     V3 px = v3(b.pos[i]) + ph * P.dt;
-    collide_all(b.colliders, P.ncoll, px, ph, P);
+    collide_all(b.colliders + P.coll_off, P.ncoll, px, ph, P);
     ppos[i] = f4(px, 0.f);
     b.phalf[i] = f4(ph, 0.f);
     if (iteration == 0 && !P.keep_initial_velocity) {

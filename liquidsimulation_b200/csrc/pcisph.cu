@@ -7,6 +7,7 @@
 #include "lsp_device.cuh"
 #include "lsp_kernels.h"
 #include "mlp.cuh"
+#include "loop_sync.cuh"
 #include "particle_ops.cuh"
 
 #include <algorithm>
@@ -110,7 +111,8 @@ __device__ __forceinline__ void warm_features(const DevParams& P, const StepBuff
     f[5] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * P.dt / P.h * 10.f;
     f[6] = w.gradrho[i] * P.h / P.rho0;
     float dist = 4.f * P.h;
-    for (int c = 0; c < P.ncoll; c++) dist = fminf(dist, fmaxf(collider_distance(b.colliders[c], x), 0.f));
+    for (int c = 0; c < P.ncoll; c++)
+        dist = fminf(dist, fmaxf(collider_distance(b.colliders[P.coll_off + c], x), 0.f));
     f[7] = dist / (4.f * P.h);
 }
 
@@ -207,51 +209,6 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 //
 // The grid barrier spins with a bounded count: past the limit it raises kErrTimeout and
 // an abort word that makes every block leave; the host reports LSP_ERR_TIMEOUT.
-
-constexpr unsigned long long kBarrierSpinLimit = 1ull << 25;
-
-struct LoopSync {
-    uint32_t count;
-    uint32_t gen;
-    uint32_t abort;
-    uint32_t pad;
-};
-
-__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(const volatile uint32_t*)p; }
-
-// Returns false when the loop must stop (a barrier gave up somewhere).
-__device__ bool grid_barrier(LoopSync* sy, DevStatus* st)
-{
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        const uint32_t g = ld_volatile(&sy->gen);
-        __threadfence();
-        uint32_t arrived = atomicAdd(&sy->count, 1u);
-        if (arrived == gridDim.x - 1) {
-            atomicExch(&sy->count, 0u);
-            __threadfence();
-            atomicAdd(&sy->gen, 1u);
-        } else {
-            unsigned long long spins = 0;
-            while (ld_volatile(&sy->gen) == g) {
-                if (ld_volatile(&sy->abort)) { ok = 0; break; }
-                if (++spins > kBarrierSpinLimit) {
-                    atomicExch(&sy->abort, 1u);
-                    atomicOr(&st->error_flags, kErrTimeout);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        if (ld_volatile(&sy->abort)) ok = 0;
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
-}
 
 __global__ void __launch_bounds__(kThreads) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt, LoopSync* sy,
                                                       uint32_t* maxerr, int first_done, int warm)

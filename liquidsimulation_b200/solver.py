@@ -323,3 +323,175 @@ def from_scene(scene, device: int = -1) -> SPHSolver:
     for c in scene.colliders:
         s.add_static_collision_object(c)
     return s
+
+
+class SceneBatch:
+    """Many independent scenes stepped together (lsp_batch_* in include/lsp.h).
+
+    The reference runs one solver object per scene; a batch holds them all in one set of
+    device arrays and advances every scene with one CUDA graph per step, the PCISPH loops of
+    all scenes in one persistent kernel. Each scene's results are bit-identical to a
+    single-scene solver given the same inputs. Scenes and colliders are added before the
+    first step."""
+
+    def __init__(self, device: int = -1):
+        self._lib = abi.load_library()
+        h = ctypes.c_void_p()
+        abi.check(self._lib, self._lib.lsp_batch_create(device, byref(h)))
+        self._h = h
+        self._counts = []
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._lib.lsp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _call(self, name, *args):
+        return abi.check(self._lib, getattr(self._lib, name)(self._h, *args))
+
+    # ------------------------------------------------------------ scenes
+    def add_scene(self, params: abi.LspParams, positions, velocities=None, domain=None) -> int:
+        x = _f32(positions).reshape(-1, 3)
+        v = None if velocities is None else _f32(velocities).reshape(-1, 3)
+        lo = hi = None
+        if domain is not None:
+            lo, hi = (np.ascontiguousarray(d, np.float32).reshape(3) for d in domain)
+        idx = c_int32()
+        self._call("lsp_batch_add_scene", byref(params), _ptr(x), _ptr(v), x.shape[0], _ptr(lo), _ptr(hi),
+                   byref(idx))
+        self._counts.append(x.shape[0])
+        return idx.value
+
+    def add_box(self, scene: int, center, half_extent, boundary: bool = False):
+        c = np.ascontiguousarray(center, np.float32)
+        h = np.ascontiguousarray(half_extent, np.float32)
+        self._call("lsp_batch_add_box", scene, _ptr(c), _ptr(h), abi.LSP_BOUNDARY if boundary else abi.LSP_OBSTACLE)
+
+    def add_sphere(self, scene: int, center, radius: float, boundary: bool = False):
+        c = np.ascontiguousarray(center, np.float32)
+        self._call("lsp_batch_add_sphere", scene, _ptr(c), c_float(radius),
+                   abi.LSP_BOUNDARY if boundary else abi.LSP_OBSTACLE)
+
+    def add_collider(self, scene: int, collider):
+        """Takes a scenes.Collider (kind 'box' or 'sphere')."""
+        if collider.kind == "box":
+            self.add_box(scene, collider.center, collider.size, collider.boundary)
+        else:
+            self.add_sphere(scene, collider.center, collider.size, collider.boundary)
+
+    def update_box(self, scene: int, index: int, center, half_extent):
+        c = np.ascontiguousarray(center, np.float32)
+        h = np.ascontiguousarray(half_extent, np.float32)
+        self._call("lsp_batch_update_box", scene, index, _ptr(c), _ptr(h))
+
+    def update_sphere(self, scene: int, index: int, center, radius: float):
+        c = np.ascontiguousarray(center, np.float32)
+        self._call("lsp_batch_update_sphere", scene, index, _ptr(c), c_float(radius))
+
+    @property
+    def scenes(self) -> int:
+        return len(self._counts)
+
+    @property
+    def total(self) -> int:
+        return int(sum(self._counts))
+
+    def count(self, scene: int) -> int:
+        return self._counts[scene]
+
+    # ------------------------------------------------------------ stepping
+    def update(self, dt: float):
+        """One step of every scene; returns the per-scene LspStepStats."""
+        st = (abi.LspStepStats * max(self.scenes, 1))()
+        self._call("lsp_batch_step", c_float(dt), st)
+        return list(st)[: self.scenes]
+
+    def set_launch(self, use_graph: bool = True, threads: int = 256, loop_blocks: int = 0):
+        self._call("lsp_batch_set_launch", int(use_graph), int(threads), int(loop_blocks))
+
+    def get_launch(self) -> dict:
+        vals = [ctypes.c_int() for _ in range(4)]
+        self._call("lsp_batch_get_launch", *(byref(v) for v in vals))
+        return dict(zip(("use_graph", "threads", "loop_blocks", "graph_active"), (v.value for v in vals)))
+
+    def autotune(self, dt: float, repeats: int = 3):
+        """Tunes the launch shape on the next step and performs that step. Returns
+        (LspBatchTuning, per-scene stats)."""
+        t = abi.LspBatchTuning()
+        st = (abi.LspStepStats * max(self.scenes, 1))()
+        self._call("lsp_batch_autotune", c_float(dt), int(repeats), byref(t), st)
+        return t, list(st)[: self.scenes]
+
+    # ------------------------------------------------------------ read-back
+    def read(self, scene: int, field: int) -> np.ndarray:
+        n = self._counts[scene]
+        shape = (n, 3) if field in abi.VECTOR_FIELDS else (n,)
+        out = np.empty(shape, np.float32)
+        self._call("lsp_batch_read_field", scene, int(field), _ptr(out), n)
+        return out
+
+    def positions(self, scene: int) -> np.ndarray:
+        return self.read(scene, abi.FIELD_POSITION)
+
+    def neighbors(self, scene: int):
+        n = self._counts[scene]
+        off = np.empty(n + 1, np.int64)
+        self._call("lsp_batch_read_neighbors", scene, _ptr(off, POINTER(c_int64)), None, n, 0)
+        idx = np.empty(max(int(off[-1]), 1), np.int32)
+        self._call("lsp_batch_read_neighbors", scene, _ptr(off, POINTER(c_int64)), _ptr(idx, POINTER(c_int32)), n,
+                   idx.size)
+        return off, idx[: int(off[-1])]
+
+    def grid(self, scene: int):
+        n = self._counts[scene]
+        dims = np.empty(3, np.int32)
+        org = np.empty(3, np.int32)
+        cells = c_int64()
+        self._call("lsp_batch_grid_info", scene, _ptr(dims, POINTER(c_int32)), _ptr(org, POINTER(c_int32)),
+                   byref(cells))
+        keys = np.empty(n, np.uint32)
+        ids = np.empty(n, np.int32)
+        start = np.empty(cells.value + 1, np.uint32)
+        self._call("lsp_batch_read_grid", scene, _ptr(keys, POINTER(c_uint32)), _ptr(ids, POINTER(c_int32)), n,
+                   _ptr(start, POINTER(c_uint32)), cells.value + 1)
+        return dims, org, keys, ids, start
+
+    def read_state(self):
+        n = self.total
+        x, v, h, o = (np.empty((n, 3), np.float32) for _ in range(4))
+        first = np.empty(n, np.int32)
+        self._call("lsp_batch_read_state", _ptr(x), _ptr(v), _ptr(h), _ptr(o), _ptr(first, POINTER(c_int32)), n)
+        return x, v, h, o, first
+
+    def write_state(self, x, v, half, old_half, first):
+        n = self.total
+        arrs = [_f32(a).reshape(n, 3) for a in (x, v, half, old_half)]
+        f = np.ascontiguousarray(first, np.int32).reshape(n)
+        self._call("lsp_batch_write_state", *(_ptr(a) for a in arrs), _ptr(f, POINTER(c_int32)), n)
+
+    def launch_count(self) -> int:
+        v = c_int64()
+        self._call("lsp_batch_launch_count", byref(v))
+        return v.value
+
+
+def batch_from_scenes(scene_list, device: int = -1) -> SceneBatch:
+    """A SceneBatch holding scenes.Scene objects in order (same dt expected)."""
+    b = SceneBatch(device)
+    for sc in scene_list:
+        k = b.add_scene(sc.params, sc.positions, sc.velocities, sc.domain)
+        for c in sc.colliders:
+            b.add_collider(k, c)
+    return b

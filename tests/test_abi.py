@@ -48,9 +48,10 @@ def test_struct_layout_matches_c(tmp_path):
 #include <stddef.h>
 #include "lsp.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(lsp_params), offsetof(lsp_params, solver),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(lsp_params), offsetof(lsp_params, solver),
          offsetof(lsp_params, pci_eta), offsetof(lsp_params, keep_initial_velocity),
-         sizeof(lsp_step_stats), offsetof(lsp_step_stats, max_neighbors));
+         sizeof(lsp_step_stats), offsetof(lsp_step_stats, max_neighbors),
+         sizeof(lsp_batch_tuning), offsetof(lsp_batch_tuning, cand_ms));
   return 0;
 }''')
     exe = tmp_path / "layout"
@@ -59,7 +60,8 @@ int main(void) {
     got = [int(x) for x in out]
     want = [ctypes.sizeof(abi.LspParams), abi.LspParams.solver.offset, abi.LspParams.pci_eta.offset,
             abi.LspParams.keep_initial_velocity.offset, ctypes.sizeof(abi.LspStepStats),
-            abi.LspStepStats.max_neighbors.offset]
+            abi.LspStepStats.max_neighbors.offset, ctypes.sizeof(abi.LspBatchTuning),
+            abi.LspBatchTuning.cand_ms.offset]
     assert got == want
 
 
@@ -88,6 +90,10 @@ def test_calls_fail_cleanly_without_device(lib):
     assert b"device" in lib.lsp_last_error()
     assert lib.lsp_step(None, ctypes.c_float(0.001), None) == abi.LSP_ERR_INVALID
     assert lib.lsp_destroy(None) == abi.LSP_OK
+    b = ctypes.c_void_p()
+    assert lib.lsp_batch_create(-1, ctypes.byref(b)) == abi.LSP_ERR_NO_DEVICE
+    assert lib.lsp_batch_step(None, ctypes.c_float(0.001), None) == abi.LSP_ERR_INVALID
+    assert lib.lsp_batch_destroy(None) == abi.LSP_OK
 
 
 def test_product_has_no_cpu_fallback():
