@@ -311,6 +311,19 @@ int lsp_batch_get_launch(const lsp_batch* b, int* use_graph, int* threads, int* 
  * per candidate, keeps the fastest shape, and leaves the batch advanced by exactly that one
  * step (results do not depend on the shape). result and stats may be NULL. */
 int lsp_batch_autotune(lsp_batch* b, float dt, int repeats, lsp_batch_tuning* result, lsp_step_stats* stats);
+/* Learned warm start for every scene of a PCISPH batch (LSP_WARM_ZERO or LSP_WARM_MLP):
+ * one network for the batch, features normalised per scene, the guess checked and rejected
+ * per scene exactly as lsp_step does. The lsp_mlp_* counterparts below act on the batch's
+ * network; train uses the features and final pressures of the last recorded step of all
+ * scenes. No counterpart in the reference. */
+int lsp_batch_set_warm_start(lsp_batch* b, int mode);
+int lsp_batch_mlp_reset(lsp_batch* b, uint64_t seed);
+int lsp_batch_mlp_set_weights(lsp_batch* b, const float* w, int n);
+int lsp_batch_mlp_get_weights(lsp_batch* b, float* w, int n);
+int lsp_batch_mlp_record(lsp_batch* b, int on);
+int lsp_batch_mlp_set_loss_asymmetry(lsp_batch* b, float over_weight);
+int lsp_batch_mlp_train(lsp_batch* b, int iterations, int batch, float lr, uint64_t seed, float* loss);
+int lsp_batch_read_features(lsp_batch* b, int32_t scene, float* out, int64_t n);
 int lsp_batch_timer_mark(lsp_batch* b, int slot);
 int lsp_batch_timer_elapsed(lsp_batch* b, int slot_a, int slot_b, float* ms);
 int lsp_batch_launch_count(const lsp_batch* b, int64_t* launches);

@@ -254,6 +254,14 @@ def _declare(lib):
         "lsp_batch_set_launch": (c_int, [c_void_p, c_int, c_int, c_int]),
         "lsp_batch_get_launch": (c_int, [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
         "lsp_batch_autotune": (c_int, [c_void_p, c_float, c_int, POINTER(LspBatchTuning), POINTER(LspStepStats)]),
+        "lsp_batch_set_warm_start": (c_int, [c_void_p, c_int]),
+        "lsp_batch_mlp_reset": (c_int, [c_void_p, ctypes.c_uint64]),
+        "lsp_batch_mlp_set_weights": (c_int, [c_void_p, fp, c_int]),
+        "lsp_batch_mlp_get_weights": (c_int, [c_void_p, fp, c_int]),
+        "lsp_batch_mlp_record": (c_int, [c_void_p, c_int]),
+        "lsp_batch_mlp_set_loss_asymmetry": (c_int, [c_void_p, c_float]),
+        "lsp_batch_mlp_train": (c_int, [c_void_p, c_int, c_int, c_float, ctypes.c_uint64, fp]),
+        "lsp_batch_read_features": (c_int, [c_void_p, c_int32, fp, c_int64]),
         "lsp_batch_timer_mark": (c_int, [c_void_p, c_int]),
         "lsp_batch_timer_elapsed": (c_int, [c_void_p, c_int, c_int, fp]),
         "lsp_batch_launch_count": (c_int, [c_void_p, i64p]),

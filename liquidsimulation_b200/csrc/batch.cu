@@ -24,6 +24,7 @@
 #include "batch_kernels.h"
 #include "loop_sync.cuh"
 #include "particle_ops.cuh"
+#include "warm_ops.cuh"
 
 #include <algorithm>
 
@@ -145,6 +146,61 @@ __global__ void __launch_bounds__(T) kb_integrate(BatchArgs a, StepBuffers b, in
     const int i = it.begin + (int)threadIdx.x;
     if (i >= it.end) return;
     integrate_one(P, b, i, add_pforce);
+}
+
+// ------------------------------------------------------------------ learned warm start
+
+template <int T>
+__global__ void __launch_bounds__(T) kb_pci_predict0(BatchArgs a, StepBuffers b)
+{
+    __shared__ DevParams P;
+    const BatchItem it = a.items[blockIdx.x];
+    stage_params(&P, a.sp, it.scene);
+    __syncthreads();
+    const int i = it.begin + (int)threadIdx.x;
+    if (i >= it.end) return;
+    pci_predict_one(P, b, i, 0, b.ppos);
+}
+
+// Iteration 0's density with the warm-start features and, with mlp, the network's guess
+// (density_first_warp); p_scale = delta * 0.01 * rho0 of the item's scene. The scene's
+// maximum |error| goes to maxerr[scene * mstride].
+template <int T>
+__global__ void __launch_bounds__(T) kb_density_first(BatchArgs a, StepBuffers b, BatchWarmArgs w)
+{
+    __shared__ DevParams P;
+    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ MlpPacked mw;
+    __shared__ uint32_t stage[T / 32][32 * 4];
+    const BatchItem it = a.items[blockIdx.x];
+    const float* tb = scene_tables(a, it.scene);
+    stage_params(&P, a.sp, it.scene);
+    stage_table(W, tb, T_W);
+    stage_table(TH, tb, T_THRESH);
+    if (w.mlp) stage_mlp(&mw, w.mlp);
+    __syncthreads();
+    const int i = it.begin + (int)threadIdx.x;
+    const float p_scale = P.delta * 0.01f * P.rho0;
+    const float e = density_first_warp(P, b, w.feat, b.hist, b.gradrho, w.mlp ? &mw : nullptr, p_scale, W, TH, i,
+                                       i < it.end, stage[threadIdx.x >> 5]);
+    uint32_t m = __float_as_uint(e);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if ((threadIdx.x & 31) == 0 && m) atomicMax(w.maxerr + (size_t)it.scene * w.mstride, m);
+}
+
+// Training targets: final pressure / p_scale of the particle's scene.
+template <int T>
+__global__ void __launch_bounds__(T) kb_targets(BatchArgs a, const float* __restrict__ pres, float* __restrict__ tgt)
+{
+    __shared__ DevParams P;
+    const BatchItem it = a.items[blockIdx.x];
+    stage_params(&P, a.sp, it.scene);
+    __syncthreads();
+    const int i = it.begin + (int)threadIdx.x;
+    if (i >= it.end) return;
+    const float p_scale = P.delta * 0.01f * P.rho0;
+    tgt[i] = pres[i] * (1.f / p_scale);
 }
 
 // ------------------------------------------------------------------ persistent loop
@@ -406,6 +462,27 @@ int launch_batch_integrate(const BatchArgs& a, const StepBuffers& b, bool add_pf
 {
     if (!a.items_count) return 0;
     LSP_BATCH_DISPATCH(a.threads, (kb_integrate<T><<<a.items_count, T, 0, s>>>(a, b, add_pforce ? 1 : 0)));
+    return 1;
+}
+
+int launch_batch_pci_predict0(const BatchArgs& a, const StepBuffers& b, cudaStream_t s)
+{
+    if (!a.items_count) return 0;
+    LSP_BATCH_DISPATCH(a.threads, (kb_pci_predict0<T><<<a.items_count, T, 0, s>>>(a, b)));
+    return 1;
+}
+
+int launch_batch_density_first(const BatchArgs& a, const StepBuffers& b, const BatchWarmArgs& w, cudaStream_t s)
+{
+    if (!a.items_count) return 0;
+    LSP_BATCH_DISPATCH(a.threads, (kb_density_first<T><<<a.items_count, T, 0, s>>>(a, b, w)));
+    return 1;
+}
+
+int launch_batch_targets(const BatchArgs& a, const float* pres, float* tgt, cudaStream_t s)
+{
+    if (!a.items_count) return 0;
+    LSP_BATCH_DISPATCH(a.threads, (kb_targets<T><<<a.items_count, T, 0, s>>>(a, pres, tgt)));
     return 1;
 }
 

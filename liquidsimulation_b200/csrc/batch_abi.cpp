@@ -216,6 +216,49 @@ int lsp_batch_autotune(lsp_batch* b, float dt, int repeats, lsp_batch_tuning* re
     return guard([&] { B(b).autotune(dt, repeats, result, stats); });
 }
 
+int lsp_batch_set_warm_start(lsp_batch* b, int mode)
+{
+    return guard([&] { B(b).set_warm_start(mode); });
+}
+
+int lsp_batch_mlp_reset(lsp_batch* b, uint64_t seed)
+{
+    return guard([&] { B(b).mlp_reset(seed); });
+}
+
+int lsp_batch_mlp_set_weights(lsp_batch* b, const float* w, int n)
+{
+    return guard([&] { B(b).mlp_set(w, n); });
+}
+
+int lsp_batch_mlp_get_weights(lsp_batch* b, float* w, int n)
+{
+    return guard([&] { B(b).mlp_get(w, n); });
+}
+
+int lsp_batch_mlp_record(lsp_batch* b, int on)
+{
+    return guard([&] { B(b).mlp_record(on != 0); });
+}
+
+int lsp_batch_mlp_set_loss_asymmetry(lsp_batch* b, float over_weight)
+{
+    return guard([&] { B(b).mlp_set_loss_asymmetry(over_weight); });
+}
+
+int lsp_batch_mlp_train(lsp_batch* b, int iterations, int batch, float lr, uint64_t seed, float* loss)
+{
+    return guard([&] {
+        float l = B(b).mlp_train(iterations, batch, lr, seed);
+        if (loss) *loss = l;
+    });
+}
+
+int lsp_batch_read_features(lsp_batch* b, int32_t scene, float* out, int64_t n)
+{
+    return guard([&] { B(b).read_features(scene, out, n); });
+}
+
 int lsp_batch_timer_mark(lsp_batch* b, int slot)
 {
     return guard([&] { B(b).timer_mark(slot); });

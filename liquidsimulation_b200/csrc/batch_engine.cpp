@@ -1,6 +1,7 @@
 // Batch of independent scenes: layout, step sequencing, CUDA graph, autotuner.
 // See batch_engine.h and batch_kernels.h.
 #include "batch_engine.h"
+#include "mlp.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -26,6 +27,7 @@ BatchEngine::BatchEngine(int device)
     if (prop.major != 10) throw Error(LSP_ERR_NO_DEVICE, "liblsp is built for sm_100a (B200); device is sm_" +
                                                              std::to_string(prop.major) + std::to_string(prop.minor));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    mlp_.init(stream_);
 }
 
 BatchEngine::~BatchEngine()
@@ -65,7 +67,8 @@ int BatchEngine::add_scene(const lsp_params& p, const float* xyz, const float* v
     const bool pci = p.solver == LSP_SOLVER_PCISPH;
     if (!sc_.empty() && pci != pcisph_) throw Error(LSP_ERR_INVALID, "all scenes of a batch use the same solver");
     if (pci && p.pci_max_iterations < 1) throw Error(LSP_ERR_INVALID, "batched PCISPH needs pci_max_iterations >= 1");
-    if (p.warm_start != LSP_WARM_ZERO) throw Error(LSP_ERR_INVALID, "batched scenes use warm_start = LSP_WARM_ZERO");
+    if (p.warm_start != LSP_WARM_ZERO)
+        throw Error(LSP_ERR_INVALID, "a batch's warm start is set for all scenes (lsp_batch_set_warm_start)");
     Scene s;
     s.prm = p;
     s.hk.build(p);
@@ -228,6 +231,7 @@ void BatchEngine::build()
     int cap0 = 16;
     for (const Scene& s : sc_) cap0 = std::max(cap0, initial_neighbor_capacity(s.prm));
     built_ = true;
+    if (features_on()) ensure_warm_buffers();
     ensure_neighbors(cap0);
     upload_colliders();
     build_items();
@@ -340,8 +344,8 @@ StepBuffers BatchEngine::buffers(int c)
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
     b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p + sc_.size();
-    b.hist = nullptr;
-    b.gradrho = nullptr;
+    b.hist = features_on() ? phist_[c].p : nullptr;
+    b.gradrho = features_on() ? gradrho_.p : nullptr;
     return b;
 }
 
@@ -363,7 +367,9 @@ int BatchEngine::enqueue_step(int c, int grid)
     g.pos_out = pos_[1 - c].p; g.vel_out = vel_[1 - c].p; g.half_out = half_[1 - c].p; g.old_out = old_[1 - c].p;
     g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
     g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
-    g.hist_in = nullptr; g.hist_out = nullptr;
+    const bool feats = features_on();
+    g.hist_in = feats ? phist_[c].p : nullptr;
+    g.hist_out = feats ? phist_[1 - c].p : nullptr;
     g.status = status_.p + S;
     launches += launch_grid_order(g, stream_);
     launches += launch_batch_neighbors(a, pos_[1 - c].p, cell_start_.p, nbr_.p, nbr_count_.p, stream_);
@@ -373,13 +379,24 @@ int BatchEngine::enqueue_step(int c, int grid)
     if (pcisph_) {
         CK(cudaMemsetAsync(loop_sync_.p, 0, 4 * sizeof(uint32_t), stream_));
         CK(cudaMemsetAsync(maxerr_.p, 0, (size_t)S * mstride_ * sizeof(uint32_t), stream_));
+        if (feats) {
+            // Iteration 0 outside the persistent kernel: predict, then density with the
+            // features and (warm start) the network's guess.
+            BatchWarmArgs w{};
+            w.feat = feat_.p;
+            w.mlp = warm_ == LSP_WARM_MLP ? mlp_.packed() : nullptr;
+            w.maxerr = maxerr_.p;
+            w.mstride = mstride_;
+            launches += launch_batch_pci_predict0(a, b, stream_);
+            launches += launch_batch_density_first(a, b, w, stream_);
+        }
         BatchLoopArgs l{};
         l.ppos_alt = ppos_alt_.p;
         l.sync = loop_sync_.p;
         l.maxerr = maxerr_.p;
         l.mstride = mstride_;
-        l.first_done = 0;
-        l.warm = 0;
+        l.first_done = feats ? 1 : 0;
+        l.warm = warm_ == LSP_WARM_MLP ? 1 : 0;
         if (!launch_batch_pci_loop(a, b, l, grid, stream_))
             throw Error(LSP_ERR_CUDA, "the cooperative launch of the batch's PCISPH loop was refused");
         launches++;
@@ -454,6 +471,7 @@ void BatchEngine::finish_step(lsp_step_stats* stats)
 {
     const int S = (int)sc_.size();
     cur_ = 1 - cur_;
+    features_valid_ = features_on();
     uint32_t errors = hstatus_[S].error_flags;
     bool not_converged = false;
     for (int s = 0; s < S; s++) {
@@ -743,6 +761,87 @@ void BatchEngine::write_state(const float* x, const float* v, const float* half,
     launch_scatter_state(s, s + 3 * n, s + 6 * n, s + 9 * n, (const int32_t*)(s + 12 * n), slot_of_id_.p,
                          pos_[cur_].p, vel_[cur_].p, half_[cur_].p, old_[cur_].p, n, stream_);
     CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// ------------------------------------------------------------------ learned warm start
+
+void BatchEngine::ensure_warm_buffers()
+{
+    if (!built_ || phist_[0].p) return;
+    activate();
+    const int64_t cap = (int64_t)pos_[0].n;
+    for (int k = 0; k < 2; k++) {
+        phist_[k].alloc(cap);
+        CK(cudaMemsetAsync(phist_[k].p, 0, cap * sizeof(float4), stream_));
+    }
+    feat_.alloc(cap * kMlpIn);
+    gradrho_.alloc(cap);
+    tgt_.alloc(cap);
+    CK(cudaMemsetAsync(feat_.p, 0, cap * kMlpIn * sizeof(float), stream_));
+    CK(cudaMemsetAsync(gradrho_.p, 0, cap * sizeof(float), stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void BatchEngine::set_warm_start(int mode)
+{
+    if (mode != LSP_WARM_ZERO && mode != LSP_WARM_MLP) throw Error(LSP_ERR_INVALID, "unknown warm_start");
+    if (mode == LSP_WARM_MLP && !sc_.empty() && !pcisph_)
+        throw Error(LSP_ERR_INVALID, "the learned warm start needs PCISPH scenes");
+    warm_ = mode;
+    drop_graphs();
+    if (features_on()) ensure_warm_buffers();
+}
+
+void BatchEngine::mlp_record(bool on)
+{
+    record_ = on;
+    drop_graphs();
+    if (features_on()) ensure_warm_buffers();
+}
+
+void BatchEngine::mlp_reset(uint64_t seed)
+{
+    activate();
+    mlp_.reset(seed);
+}
+
+void BatchEngine::mlp_set(const float* w, int n)
+{
+    activate();
+    mlp_.set(w, n);
+}
+
+void BatchEngine::mlp_get(float* w, int n)
+{
+    activate();
+    mlp_.get(w, n);
+}
+
+void BatchEngine::mlp_set_loss_asymmetry(float w) { mlp_.set_over_weight(w); }
+
+float BatchEngine::mlp_train(int iterations, int batch, float lr, uint64_t seed)
+{
+    if (!built_ || !features_valid_)
+        throw Error(LSP_ERR_STATE, "mlp_train needs a PCISPH step that recorded features (lsp_batch_mlp_record)");
+    if (iterations <= 0 || batch <= 0) throw Error(LSP_ERR_INVALID, "iterations and batch must be > 0");
+    activate();
+    launch_batch_targets(args(), pres_.p, tgt_.p, stream_);
+    CK(cudaGetLastError());
+    return mlp_.train(feat_.p, tgt_.p, n_, iterations, batch, lr, seed);
+}
+
+void BatchEngine::read_features(int scene, float* out, int64_t n)
+{
+    check_scene(scene);
+    const Scene& s = sc_[scene];
+    if (!out || n != s.n) throw Error(LSP_ERR_INVALID, "read_features: n must equal the scene's particle count");
+    if (!features_valid_) throw Error(LSP_ERR_STATE, "no step has recorded features");
+    activate();
+    stage((size_t)n * kMlpIn);
+    launch_gather_rows(feat_.p, kMlpIn, slot_of_id_.p + s.base, stage_.p, n, stream_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, stage_.p, (size_t)n * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
 }
 

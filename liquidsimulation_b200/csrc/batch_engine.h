@@ -48,6 +48,18 @@ public:
     float timer_elapsed(int a, int b);
     int64_t launch_count() const { return launches_; }
 
+    // Learned warm start of every PCISPH scene (one network for the batch; features are
+    // normalised per scene).
+    void set_warm_start(int mode);
+    void mlp_reset(uint64_t seed);
+    void mlp_set(const float* w, int n);
+    void mlp_get(float* w, int n);
+    void mlp_record(bool on);
+    void mlp_set_loss_asymmetry(float w);
+    // Adam steps on the features and final pressures of the last recorded step.
+    float mlp_train(int iterations, int batch, float lr, uint64_t seed);
+    void read_features(int scene, float* out, int64_t n);
+
 private:
     struct Scene {
         lsp_params prm{};
@@ -80,6 +92,8 @@ private:
     BatchArgs args();
     void stage(size_t floats);
     void check_scene(int scene) const;
+    bool features_on() const { return pcisph_ && (record_ || warm_ == LSP_WARM_MLP); }
+    void ensure_warm_buffers();
 
     int dev_ = 0;
     cudaStream_t stream_ = nullptr;
@@ -116,6 +130,12 @@ private:
 
     cudaEvent_t marks_[16] = {};
     int64_t launches_ = 0;
+
+    int warm_ = LSP_WARM_ZERO;
+    bool record_ = false, features_valid_ = false;
+    DevArray<float4> phist_[2];   // pressure history (p_{n-1}, p_{n-2}, p_{n-3})
+    DevArray<float> feat_, gradrho_, tgt_;
+    MlpModel mlp_;
 };
 
 }  // namespace lsp

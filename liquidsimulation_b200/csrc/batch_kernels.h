@@ -51,6 +51,19 @@ int launch_batch_nonpressure(const BatchArgs& a, const StepBuffers& b, cudaStrea
 int launch_batch_sph_pressure(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
 int launch_batch_integrate(const BatchArgs& a, const StepBuffers& b, bool add_pforce, cudaStream_t s);
 
+// Learned warm start of a batch: iteration 0's predict, then its density pass with the
+// features (b.hist, b.gradrho) and, with mlp, the network's guess; per-scene maximum
+// |error| to maxerr[scene * mstride]. Training targets p / p_scale per scene.
+struct BatchWarmArgs {
+    float* feat;             // [n][8] features, written
+    const MlpPacked* mlp;    // null: features only (recording a plain step)
+    uint32_t* maxerr;
+    int mstride;
+};
+int launch_batch_pci_predict0(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
+int launch_batch_density_first(const BatchArgs& a, const StepBuffers& b, const BatchWarmArgs& w, cudaStream_t s);
+int launch_batch_targets(const BatchArgs& a, const float* pres, float* tgt, cudaStream_t s);
+
 // The PCISPH loop of every scene in one cooperative launch of `grid` blocks of a.threads
 // threads (grid <= batch_loop_max_blocks). Scenes iterate in lockstep rounds separated by
 // grid barriers, each with its own iteration count, convergence test and warm-start check.

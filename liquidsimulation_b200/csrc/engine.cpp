@@ -142,7 +142,7 @@ Engine::Engine(const lsp_params& p, int device)
     maxerr_.alloc(kMaxIterationsCap);
     prm_ = p;
     derive();
-    mlp_reset(0);
+    mlp_.init(stream_);
 }
 
 Engine::~Engine()
@@ -546,7 +546,7 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         w.feat = feat_.p;
         w.hist = phist_[cur_].p;
         w.gradrho = gradrho_.p;
-        w.mlp = warm ? reinterpret_cast<const MlpPacked*>(mlp_packed_.p) : nullptr;
+        w.mlp = warm ? mlp_.packed() : nullptr;
         w.p_scale = P.delta * 0.01f * P.rho0;
         last_p_scale_ = w.p_scale;
         features_valid_ = true;
@@ -875,66 +875,25 @@ void Engine::ensure_warm_buffers()
     CK(cudaMemsetAsync(gradrho_.p, 0, cap_ * sizeof(float), stream_));
 }
 
-void Engine::mlp_repack()
-{
-    launch_mlp_pack(mlp_master_.p, reinterpret_cast<MlpPacked*>(mlp_packed_.p), stream_);
-    CK(cudaGetLastError());
-}
-
-// Uniform(-a, a) weights with a = sqrt(6 / (fan_in + fan_out)), zero biases, the output
-// layer scaled down so an untrained network guesses close to zero.
 void Engine::mlp_reset(uint64_t seed)
 {
     activate();
-    std::vector<float> w(kMlpParams, 0.f);
-    std::mt19937_64 rng(seed);
-    auto fill = [&](int off, int fin, int fout, float scale) {
-        std::uniform_real_distribution<float> u(-1.f, 1.f);
-        float a = scale * std::sqrt(6.f / (float)(fin + fout));
-        for (int i = 0; i < fin * fout; i++) w[off + i] = a * u(rng);
-    };
-    fill(kOffW1, kMlpIn, kMlpHidden, 1.f);
-    fill(kOffW2, kMlpHidden, kMlpHidden, 1.f);
-    fill(kOffW3, kMlpHidden, 1, 0.1f);
-    if (!mlp_master_.p) {
-        mlp_master_.alloc(kMlpParams);
-        mlp_m1_.alloc(kMlpParams);
-        mlp_m2_.alloc(kMlpParams);
-        mlp_grad_.alloc(kMlpParams);
-        mlp_loss_.alloc(1);
-        mlp_packed_.alloc(sizeof(MlpPacked) / 4);
-    }
-    mlp_set(w.data(), kMlpParams);
+    mlp_.reset(seed);
 }
 
 void Engine::mlp_set(const float* w, int n)
 {
-    if (!w || n != kMlpParams) throw Error(LSP_ERR_INVALID, "MLP parameter vector must hold 1377 floats");
     activate();
-    CK(cudaMemcpyAsync(mlp_master_.p, w, kMlpParams * sizeof(float), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemsetAsync(mlp_m1_.p, 0, kMlpParams * sizeof(float), stream_));
-    CK(cudaMemsetAsync(mlp_m2_.p, 0, kMlpParams * sizeof(float), stream_));
-    mlp_step_ = 0;
-    mlp_repack();
-    CK(cudaStreamSynchronize(stream_));
+    mlp_.set(w, n);
 }
 
 void Engine::mlp_get(float* w, int n)
 {
-    if (!w || n != kMlpParams) throw Error(LSP_ERR_INVALID, "MLP parameter vector must hold 1377 floats");
     activate();
-    CK(cudaMemcpyAsync(w, mlp_master_.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    mlp_.get(w, n);
 }
 
-// Weight of the squared error of over-estimates in training. With a zero negative-pressure
-// factor PCISPH only ever adds pressure, so a guess that is too high cannot be corrected
-// within the step; weighting those errors up biases the guess low.
-void Engine::mlp_set_loss_asymmetry(float w)
-{
-    if (!(w >= 1.f) || !std::isfinite(w)) throw Error(LSP_ERR_INVALID, "loss asymmetry must be >= 1");
-    mlp_over_weight_ = w;
-}
+void Engine::mlp_set_loss_asymmetry(float w) { mlp_.set_over_weight(w); }
 
 void Engine::mlp_record(bool on)
 {
@@ -943,71 +902,27 @@ void Engine::mlp_record(bool on)
 }
 
 // Adam steps on the features and final pressures of the last step (targets p / p_scale).
+// Adam steps on the features and final pressures of the last step (targets p / p_scale).
 float Engine::mlp_train(int iterations, int batch, float lr, uint64_t seed)
 {
     if (!features_valid_ || !stepped_ || n_ == 0)
         throw Error(LSP_ERR_STATE, "mlp_train needs a PCISPH step that recorded features (lsp_mlp_record)");
     if (iterations <= 0 || batch <= 0) throw Error(LSP_ERR_INVALID, "iterations and batch must be > 0");
     activate();
-    batch = (int)std::min<int64_t>(batch, n_);
-    const int rows = mlp_grad_rows(batch);
-    if (mlp_partial_.n < (size_t)rows * kMlpParams) mlp_partial_.alloc((size_t)rows * kMlpParams);
-    if (mlp_loss_part_.n < (size_t)rows) mlp_loss_part_.alloc(rows);
-    if (mlp_idx_.n < (size_t)batch) mlp_idx_.alloc(batch);
     launch_scale(pres_.p, tgt_.p, n_, 1.f / last_p_scale_, stream_);
-    for (int it = 0; it < iterations; it++) {
-        launch_random_indices(mlp_idx_.p, batch, (int)n_, seed * 1000003ull + (uint64_t)it, stream_);
-        launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), feat_.p, tgt_.p, mlp_idx_.p, batch,
-                        mlp_over_weight_, mlp_partial_.p, mlp_loss_part_.p, stream_);
-        mlp_step_++;
-        launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, nullptr,
-                        mlp_loss_.p, lr, mlp_step_, 1, stream_);
-        mlp_repack();
-    }
-    CK(cudaGetLastError());
-    float loss = 0.f;
-    CK(cudaMemcpyAsync(&loss, mlp_loss_.p, sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    return loss / (float)batch;
+    return mlp_.train(feat_.p, tgt_.p, n_, iterations, batch, lr, seed);
 }
 
 void Engine::mlp_forward(const float* feat, int64_t n, float* out)
 {
-    if (!feat || !out || n <= 0 || n > (1 << 26)) throw Error(LSP_ERR_INVALID, "mlp_forward: bad arguments");
     activate();
-    if (mlp_io_.n < (size_t)n * (kMlpIn + 2)) mlp_io_.alloc((size_t)n * (kMlpIn + 2));
-    float* df = mlp_io_.p;
-    float* dout = df + n * kMlpIn;
-    CK(cudaMemcpyAsync(df, feat, n * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, stream_));
-    launch_mlp_infer(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dout, (int)n, stream_);
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(out, dout, n * sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
+    mlp_.forward(feat, n, out);
 }
 
-// Gradient of 1/(2n) sum (y - t)^2 over the given batch at the current parameters.
 float Engine::mlp_gradient(const float* feat, const float* target, int64_t n, float* grad)
 {
-    if (!feat || !target || !grad || n <= 0 || n > (1 << 26)) throw Error(LSP_ERR_INVALID, "mlp_gradient: bad arguments");
     activate();
-    if (mlp_io_.n < (size_t)n * (kMlpIn + 2)) mlp_io_.alloc((size_t)n * (kMlpIn + 2));
-    float* df = mlp_io_.p;
-    float* dt = df + n * kMlpIn;
-    CK(cudaMemcpyAsync(df, feat, n * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, stream_));
-    CK(cudaMemcpyAsync(dt, target, n * sizeof(float), cudaMemcpyHostToDevice, stream_));
-    const int rows = mlp_grad_rows((int)n);
-    if (mlp_partial_.n < (size_t)rows * kMlpParams) mlp_partial_.alloc((size_t)rows * kMlpParams);
-    if (mlp_loss_part_.n < (size_t)rows) mlp_loss_part_.alloc(rows);
-    launch_mlp_grad(reinterpret_cast<const MlpPacked*>(mlp_packed_.p), df, dt, nullptr, (int)n, 1.f,
-                    mlp_partial_.p, mlp_loss_part_.p, stream_);
-    launch_mlp_adam(mlp_partial_.p, mlp_loss_part_.p, rows, mlp_master_.p, mlp_m1_.p, mlp_m2_.p, mlp_grad_.p,
-                    mlp_loss_.p, 0.f, 1, 0, stream_);
-    CK(cudaGetLastError());
-    float loss = 0.f;
-    CK(cudaMemcpyAsync(grad, mlp_grad_.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(&loss, mlp_loss_.p, sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaStreamSynchronize(stream_));
-    return loss / (float)n;
+    return mlp_.gradient(feat, target, n, grad);
 }
 
 void Engine::read_features(float* out, int64_t n)
@@ -1020,14 +935,5 @@ void Engine::read_features(float* out, int64_t n)
     CK(cudaMemcpyAsync(out, stage_.p, (size_t)n * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaStreamSynchronize(stream_));
 }
-
-template struct DevArray<float4>;
-template struct DevArray<float>;
-template struct DevArray<uint32_t>;
-template struct DevArray<int32_t>;
-template struct DevArray<int64_t>;
-template struct DevArray<int2>;
-template struct DevArray<Collider>;
-template struct DevArray<DevStatus>;
 
 }  // namespace lsp

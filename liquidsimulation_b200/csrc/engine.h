@@ -10,14 +10,11 @@
 #include <cuda_runtime.h>
 
 #include "../../include/lsp.h"
+#include "host_util.h"
 #include "lsp_kernels.h"
+#include "mlp_model.h"
 
 namespace lsp {
-
-struct Error : std::runtime_error {
-    int code;
-    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
 
 // Reference-identical host arithmetic (compiled with -ffp-contract=off).
 struct HostKernels {
@@ -27,42 +24,6 @@ struct HostKernels {
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;
 };
-
-template <typename T>
-struct DevArray {
-    T* p = nullptr;
-    size_t n = 0;
-    void alloc(size_t count)
-    {
-        release();
-        if (count == 0) return;
-        cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
-        if (e != cudaSuccess) {
-            p = nullptr;
-            throw Error(e == cudaErrorMemoryAllocation ? LSP_ERR_CAPACITY : LSP_ERR_CUDA,
-                        std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
-                            cudaGetErrorString(e));
-        }
-        n = count;
-    }
-    void release()
-    {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    DevArray() = default;
-    DevArray(const DevArray&) = delete;
-    DevArray& operator=(const DevArray&) = delete;
-    ~DevArray() { release(); }
-};
-
-#define LSP_CK(call)                                                                              \
-    do {                                                                                          \
-        cudaError_t e_ = (call);                                                                  \
-        if (e_ != cudaSuccess)                                                                    \
-            throw ::lsp::Error(LSP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
 
 // Parameter checks shared by single scenes and batches (LSP_ERR_INVALID on failure).
 void validate_params(const lsp_params& p);
@@ -129,7 +90,7 @@ public:
     void read_features(float* out, int64_t n);
 
     // Device copy of the fragment-ordered MLP weights (MlpPacked).
-    const void* mlp_packed_device() const { return mlp_packed_.p; }
+    const void* mlp_packed_device() const { return mlp_.packed(); }
 
     cudaStream_t stream() const { return stream_; }
     int device() const { return dev_; }
@@ -201,16 +162,11 @@ private:
     // Learned warm start state.
     bool features_on() const;
     void ensure_warm_buffers();
-    void mlp_repack();
     bool record_ = false, features_valid_ = false;
     float last_p_scale_ = 1.f;
     DevArray<float4> phist_[2];   // pressure history (p_{n-1}, p_{n-2}, p_{n-3})
     DevArray<float> feat_, gradrho_, tgt_;
-    DevArray<float> mlp_master_, mlp_m1_, mlp_m2_, mlp_partial_, mlp_loss_part_, mlp_grad_, mlp_loss_, mlp_io_;
-    DevArray<int32_t> mlp_idx_;
-    DevArray<uint32_t> mlp_packed_;
-    int mlp_step_ = 0;
-    float mlp_over_weight_ = 1.f;
+    MlpModel mlp_;
 };
 
 }  // namespace lsp

@@ -9,6 +9,7 @@
 #include "mlp.cuh"
 #include "loop_sync.cuh"
 #include "particle_ops.cuh"
+#include "warm_ops.cuh"
 
 #include <algorithm>
 
@@ -78,47 +79,11 @@ void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 }
 
 // ------------------------------------------------------------------ learned warm start
-//
-// Features of particle i at iteration 0 (all dimensionless):
-//   f0 predicted density error at zero pressure, in % of rho0 (clamped to +-50)
-//   f1 f2 f3  pressures of the previous three steps / p_scale
-//   f4 neighbour count / 32      f5 |v| dt / h * 10      f6 |grad rho| h / rho0
-//   f7 distance to the nearest collider surface / (4 h), clamped to [0, 1]
-// p_scale = delta * 0.01 * rho0 is the pressure one correction assigns to a 1 % error.
-
-__device__ __forceinline__ float collider_distance(const Collider& o, V3 x)
-{
-    V3 d = v3(fabsf(x.x - o.cx), fabsf(x.y - o.cy), fabsf(x.z - o.cz));
-    if (o.sphere) {
-        float r = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z);
-        return o.boundary ? o.radius - r : r - o.radius;
-    }
-    if (o.boundary) return fminf(fminf(o.hx - d.x, o.hy - d.y), o.hz - d.z);
-    return fmaxf(fmaxf(d.x - o.hx, d.y - o.hy), d.z - o.hz);
-}
-
-__device__ __forceinline__ void warm_features(const DevParams& P, const StepBuffers& b, const WarmArgs& w, int i,
-                                              float pd, int cnt, float (&f)[kMlpIn])
-{
-    const float4 hs = w.hist[i];
-    const float4 v = b.vel[i];
-    const V3 x = v3(b.pos[i]);
-    f[0] = fminf(fmaxf((pd - P.rho0) / (0.01f * P.rho0), -50.f), 50.f);
-    f[1] = hs.x / w.p_scale;
-    f[2] = hs.y / w.p_scale;
-    f[3] = hs.z / w.p_scale;
-    f[4] = (float)cnt * (1.f / 32.f);
-    f[5] = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z) * P.dt / P.h * 10.f;
-    f[6] = w.gradrho[i] * P.h / P.rho0;
-    float dist = 4.f * P.h;
-    for (int c = 0; c < P.ncoll; c++)
-        dist = fminf(dist, fmaxf(collider_distance(b.colliders[P.coll_off + c], x), 0.f));
-    f[7] = dist / (4.f * P.h);
-}
 
 // Iteration 0's density pass (PCISPHSolver.cpp:100-126 with p starting at 0) that also
 // computes the warm-start features and, with w.mlp, replaces the pressure of this first
-// correction by the network's guess. Without w.mlp its results are those of the plain pass.
+// correction by the network's guess (warm_ops.cuh). Without w.mlp its results are those of
+// the plain pass.
 __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, StepBuffers b, WarmArgs w)
 {
     __shared__ float W[kTableSize], TH[kTableSize + 1];
@@ -127,51 +92,11 @@ __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, Ste
     __shared__ float wmax[kThreads / 32];
     for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
     stage_thresholds(TH, b.tables);
-    if (w.mlp) {
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(w.mlp);
-        uint32_t* dst = reinterpret_cast<uint32_t*>(&mw);
-        for (int t = threadIdx.x; t < (int)(sizeof(MlpPacked) / 4); t += blockDim.x) dst[t] = src[t];
-    }
+    if (w.mlp) stage_mlp(&mw, w.mlp);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < P.n;
-    float a = 0.f, pd = 0.f, p = 0.f;
-    float f[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (valid) {
-        const V3 xi = v3(b.ppos[i]);
-        const int cnt = __ldg(b.nbr_count + i);
-        float sum = 0.f;
-        for_each_neighbor<4>(b.nbr + i, P.nbr_stride, cnt, [&](int j) { return b.ppos[j]; },
-                             [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
-        pd = P.mass * sum;
-        float er = pd - P.rho0;
-        float pp = P.delta * er;
-        if (pp < 0.f) {
-            er *= P.neg;
-            pp *= P.neg;
-        }
-        p = 0.f + pp;
-        b.prho[i] = pd;
-        b.err[i] = er;
-        a = fabsf(er);
-        a = a == a ? a : 0.f;
-        warm_features(P, b, w, i, pd, cnt, f);
-        if (w.feat) {
-#pragma unroll
-            for (int c = 0; c < kMlpIn; c++) w.feat[(int64_t)i * kMlpIn + c] = f[c];
-        }
-    }
-    if (w.mlp) {
-        float y = mlp_warp_eval(mw, f, stage[threadIdx.x >> 5]);
-        if (valid) {
-            p = y * w.p_scale;
-            if (P.neg == 0.f && p < 0.f) p = 0.f;
-        }
-    }
-    if (valid) {
-        b.pres[i] = p;
-        reinterpret_cast<float*>(b.ppos + i)[3] = p / (pd * pd);
-    }
+    const float a = density_first_warp(P, b, w.feat, w.hist, w.gradrho, w.mlp ? &mw : nullptr, w.p_scale, W, TH, i,
+                                       i < P.n, stage[threadIdx.x >> 5]);
     uint32_t m = __float_as_uint(a);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));

@@ -434,6 +434,40 @@ class SceneBatch:
         self._call("lsp_batch_autotune", c_float(dt), int(repeats), byref(t), st)
         return t, list(st)[: self.scenes]
 
+    # ------------------------------------------------------------ learned warm start
+    def set_warm_start(self, mode: int):
+        self._call("lsp_batch_set_warm_start", int(mode))
+
+    def mlp_reset(self, seed: int = 0):
+        self._call("lsp_batch_mlp_reset", ctypes.c_uint64(seed))
+
+    def mlp_set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        self._call("lsp_batch_mlp_set_weights", _ptr(w), w.size)
+
+    def mlp_get_weights(self) -> np.ndarray:
+        w = np.empty(abi.MLP_PARAMS, np.float32)
+        self._call("lsp_batch_mlp_get_weights", _ptr(w), w.size)
+        return w
+
+    def mlp_record(self, on: bool = True):
+        self._call("lsp_batch_mlp_record", int(on))
+
+    def mlp_set_loss_asymmetry(self, over_weight: float):
+        self._call("lsp_batch_mlp_set_loss_asymmetry", c_float(over_weight))
+
+    def mlp_train(self, iterations: int = 4, batch: int = 65536, lr: float = 1e-3, seed: int = 0) -> float:
+        loss = c_float()
+        self._call("lsp_batch_mlp_train", int(iterations), int(batch), c_float(lr), ctypes.c_uint64(seed),
+                   byref(loss))
+        return loss.value
+
+    def read_features(self, scene: int) -> np.ndarray:
+        n = self._counts[scene]
+        out = np.empty((n, abi.MLP_FEATURES), np.float32)
+        self._call("lsp_batch_read_features", scene, _ptr(out), n)
+        return out
+
     # ------------------------------------------------------------ read-back
     def read(self, scene: int, field: int) -> np.ndarray:
         n = self._counts[scene]

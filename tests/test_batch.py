@@ -231,3 +231,68 @@ def test_state_roundtrip_and_errors():
     with pytest.raises(abi.LspError):
         fresh.set_launch(True, 192, 0)
     fresh.close()
+
+
+def _trained_weights(sc, steps=8):
+    trainer = from_scene(sc)
+    trainer.mlp_record(True)
+    for t in range(steps):
+        trainer.update(sc.dt)
+        trainer.mlp_train(iterations=10, batch=4096, lr=3e-3, seed=t)
+    w = trainer.mlp_get_weights()
+    trainer.close()
+    return w
+
+
+@pytest.mark.parametrize("guess", ["trained", "absurd"])
+def test_batch_warm_start_matches_single_scenes(guess):
+    """Learned warm start in a batch: per scene, the features, the kept/rejected decision,
+    the iteration count and every field equal the single-scene warm start's bits."""
+    from oracle import mlp_oracle as M
+    scs = small_batch(seed=13, count=4)
+    if guess == "trained":
+        w = _trained_weights(scs[0])
+    else:
+        w = M.init(1).astype(np.float32)
+        w[M.OFF["b3"]] = 400.0   # every guess raises the error: every scene restarts from zero
+    batch = batch_from_scenes(scs)
+    batch.mlp_set_weights(w)
+    batch.set_warm_start(abi.LSP_WARM_MLP)
+    singles = [from_scene(sc) for sc in scs]
+    for s in singles:
+        s.mlp_set_weights(w)
+        s.set_warm_start(abi.LSP_WARM_MLP)
+    dt = scs[0].dt
+    kept = 0
+    for step in range(5):
+        sb = batch.update(dt)
+        for k, s in enumerate(singles):
+            ss = s.update(dt)
+            assert (sb[k].iterations, sb[k].warm_start_used, sb[k].converged) == \
+                   (ss.iterations, ss.warm_start_used, ss.converged), (step, k)
+            kept += sb[k].warm_start_used
+            compare_scene(batch, k, s, grid=False, nbrs=(step == 4), tag=f"{guess} step {step}")
+            assert np.array_equal(bits(batch.read_features(k)), bits(s.read_features())), (step, k)
+    if guess == "absurd":
+        assert kept == 0
+    close_all(batch, singles)
+
+
+def test_batch_records_and_trains():
+    scs = small_batch(seed=14, count=4)
+    batch = batch_from_scenes(scs)
+    batch.mlp_record(True)
+    batch.mlp_set_loss_asymmetry(4.0)
+    dt = scs[0].dt
+    losses = []
+    for step in range(10):
+        batch.update(dt)
+        losses.append(batch.mlp_train(iterations=10, batch=8192, lr=3e-3, seed=step))
+    assert np.isfinite(losses).all() and losses[-1] < losses[0]
+    f = batch.read_features(2)
+    assert f.shape == (scs[2].n, 8) and np.isfinite(f).all()
+    batch.mlp_record(False)
+    batch.set_warm_start(abi.LSP_WARM_MLP)
+    st = batch.update(dt)
+    assert all(s.converged for s in st)
+    batch.close()
