@@ -178,6 +178,17 @@ def test_injected_state(oracle_mod):
     gpu.close()
 
 
+def test_speed_squared_field(oracle_mod):
+    """The headless colour source: |v|^2 as Vector3D::squareMagnitude rounds it
+    (Vector3D.cpp:55-58, read by SPHParticleDrawable.cpp:10-27), from the oracle's v."""
+    sc = scenes.small_box_scene(n_side=(8, 8, 8))
+    gpu, orc = run_pair(oracle_mod, sc, 3, check_neighbors=False)
+    v = orc.get(abi.FIELD_VELOCITY).astype(np.float32)
+    want = (v[:, 0] * v[:, 0] + v[:, 1] * v[:, 1]) + v[:, 2] * v[:, 2]
+    assert bits_equal(gpu.read(abi.FIELD_SPEED_SQUARED), want)
+    gpu.close()
+
+
 def test_add_particles_mid_run_and_moving_collider(oracle_mod):
     sc = scenes.small_box_scene(n_side=(8, 8, 8))
     gpu = from_scene(sc)
