@@ -155,4 +155,72 @@ public:
     void setMaxDensityErrorRatio(float v) { edit([&](lsp_params& p) { p.pci_eta = v; }); }
 };
 
+// Many independent scenes stepped together (lsp_batch_* in lsp.h): what an application
+// would otherwise do with one solver object per scene, each updated in turn. Scenes and
+// their colliders are added before the first update; each scene's results equal those of
+// its own solver object.
+class SceneBatch {
+public:
+    explicit SceneBatch(int device = -1) { check(lsp_batch_create(device, &b_)); }
+    ~SceneBatch()
+    {
+        if (b_) lsp_batch_destroy(b_);
+    }
+    SceneBatch(const SceneBatch&) = delete;
+    SceneBatch& operator=(const SceneBatch&) = delete;
+
+    // A scene from parameters (lsp_params_default + edits) and particles in caller order.
+    // domain_lo / domain_hi may both be null (grid box from the boundary colliders).
+    int addScene(const lsp_params& params, const float* xyz, const float* vel, int64_t n,
+                 const float* domain_lo = nullptr, const float* domain_hi = nullptr)
+    {
+        int32_t k = -1;
+        check(lsp_batch_add_scene(b_, &params, xyz, vel, n, domain_lo, domain_hi, &k));
+        counts_.push_back(n);
+        return k;
+    }
+    void addStaticCollisionBox(int scene, Vec3 center, Vec3 halfExtent, CollisionType type)
+    {
+        float c[3] = {center.x, center.y, center.z}, h[3] = {halfExtent.x, halfExtent.y, halfExtent.z};
+        check(lsp_batch_add_box(b_, scene, c, h, (int)type));
+    }
+    void addStaticCollisionSphere(int scene, Vec3 center, float radius, CollisionType type)
+    {
+        float c[3] = {center.x, center.y, center.z};
+        check(lsp_batch_add_sphere(b_, scene, c, radius, (int)type));
+    }
+    // One step of every scene; per-scene statistics.
+    std::vector<lsp_step_stats> update(float deltaTime)
+    {
+        std::vector<lsp_step_stats> st(counts_.size());
+        check(lsp_batch_step(b_, deltaTime, st.data()));
+        return st;
+    }
+    // Chooses the launch shape on the next step and performs that step.
+    lsp_batch_tuning autotune(float deltaTime, int repeats = 3)
+    {
+        lsp_batch_tuning t{};
+        std::vector<lsp_step_stats> st(counts_.size());
+        check(lsp_batch_autotune(b_, deltaTime, repeats, &t, st.data()));
+        return t;
+    }
+    int sceneCount() const { return (int)counts_.size(); }
+    int64_t particleCount(int scene) const { return counts_.at(scene); }
+    std::vector<float> positions(int scene) { return field(scene, LSP_FIELD_POSITION, 3); }
+    std::vector<float> velocities(int scene) { return field(scene, LSP_FIELD_VELOCITY, 3); }
+    std::vector<float> densities(int scene) { return field(scene, LSP_FIELD_DENSITY, 1); }
+    std::vector<float> field(int scene, int id, int comps)
+    {
+        int64_t n = particleCount(scene);
+        std::vector<float> out((size_t)n * comps);
+        check(lsp_batch_read_field(b_, scene, id, out.data(), n));
+        return out;
+    }
+    lsp_batch* handle() { return b_; }
+
+private:
+    lsp_batch* b_ = nullptr;
+    std::vector<int64_t> counts_;
+};
+
 }  // namespace lsp
