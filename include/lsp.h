@@ -238,6 +238,19 @@ int lsp_profile(lsp_solver* s, int enable);
 int lsp_profile_read(lsp_solver* s, double* ms, int64_t* launches, int capacity);
 /* Kernels this solver has launched since creation. */
 int lsp_launch_count(const lsp_solver* s, int64_t* launches);
+/* ---- state files: save / resume, golden files ----
+ * One binary file per scene: parameters, colliders, grid box, the caller-order state
+ * (x, v, v_half, v_half_old, first-step flags), the warm-start pressure history when it
+ * exists and the MLP weights (layout at the top of csrc/state_io.cpp). Loading replaces
+ * the handle's parameters, particles, colliders and grid box; a resumed run continues
+ * bit-identically to the run that was saved (the optimiser's Adam moments are not saved).
+ * `seed` is the caller's label of the scene, stored as given. No counterpart in the
+ * reference (it has no persistence). */
+int lsp_save_state(lsp_solver* s, const char* path, uint64_t seed);
+int lsp_load_state(lsp_solver* s, const char* path);
+/* Reads only the header (no device needed): any output may be NULL. */
+int lsp_state_file_info(const char* path, lsp_params* params, int64_t* n, int32_t* colliders, uint64_t* seed);
+
 /* Page-locked host memory for asynchronous copies (cudaMallocHost / cudaFreeHost). */
 int lsp_host_alloc(size_t bytes, void** out);
 int lsp_host_free(void* p);

@@ -232,6 +232,9 @@ def _declare(lib):
         "lsp_mlp_forward": (c_int, [S, fp, c_int64, fp]),
         "lsp_mlp_gradient": (c_int, [S, fp, fp, c_int64, fp, fp]),
         "lsp_read_features": (c_int, [S, fp, c_int64]),
+        "lsp_save_state": (c_int, [S, c_char_p, ctypes.c_uint64]),
+        "lsp_load_state": (c_int, [S, c_char_p]),
+        "lsp_state_file_info": (c_int, [c_char_p, POINTER(LspParams), i64p, i32p, POINTER(ctypes.c_uint64)]),
         # batches of independent scenes
         "lsp_batch_create": (c_int, [c_int, POINTER(c_void_p)]),
         "lsp_batch_destroy": (c_int, [c_void_p]),

@@ -808,6 +808,42 @@ void Engine::write_state(const float* x, const float* v, const float* half, cons
     if (domain_from_particles_) grid_valid_ = false;
 }
 
+bool Engine::domain(float lo[3], float hi[3]) const
+{
+    std::memcpy(lo, dom_lo_, sizeof(dom_lo_));
+    std::memcpy(hi, dom_hi_, sizeof(dom_hi_));
+    return domain_user_;
+}
+
+void Engine::read_history(float* out, int64_t n)
+{
+    if (!out || n != n_) throw Error(LSP_ERR_INVALID, "read_history: n must equal the particle count");
+    if (n == 0) return;
+    if (!phist_[cur_].p) {
+        std::memset(out, 0, (size_t)n * 3 * sizeof(float));
+        return;
+    }
+    activate();
+    stage((size_t)n * 3);
+    launch_gather_field(phist_[cur_].p, 3, 0, slot_of_id_.p, stage_.p, n, stream_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, stage_.p, (size_t)n * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::write_history(const float* in, int64_t n)
+{
+    if (!in || n != n_) throw Error(LSP_ERR_INVALID, "write_history: n must equal the particle count");
+    if (n == 0) return;
+    activate();
+    ensure_warm_buffers();
+    stage((size_t)n * 3);
+    CK(cudaMemcpyAsync(stage_.p, in, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    launch_scatter_vec(stage_.p, slot_of_id_.p, phist_[cur_].p, n, stream_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
 void Engine::read_neighbors(int64_t* offsets, int32_t* index, int64_t n, int64_t capacity)
 {
     if (n != n_ || !offsets) throw Error(LSP_ERR_INVALID, "read_neighbors: bad arguments");

@@ -58,6 +58,19 @@ public:
     void remove_colliders();
     const std::vector<Collider>& colliders() const { return cols_; }
     void set_domain(const float lo[3], const float hi[3]);
+    // The user grid box, if one was set (lsp_set_domain); clear_domain returns to the
+    // boundary-collider / particle-bounds rule.
+    bool domain(float lo[3], float hi[3]) const;
+    void clear_domain()
+    {
+        domain_user_ = false;
+        grid_valid_ = false;
+    }
+    // Warm-start pressure history (p_{n-1}, p_{n-2}, p_{n-3}) in caller order, float[3n];
+    // has_history is false while the warm-start buffers do not exist (all zero then).
+    bool has_history() const { return phist_[cur_].p != nullptr; }
+    void read_history(float* out, int64_t n);
+    void write_history(const float* in, int64_t n);
 
     void step(float dt, lsp_step_stats* st);
     void step_many(float dt, int steps, lsp_step_stats* st);

@@ -95,6 +95,19 @@ void launch_scatter_state(const float* x, const float* v, const float* half, con
                                                                oldv, n);
 }
 
+__global__ void k_scatter_vec(const float* __restrict__ in, const int32_t* __restrict__ slot_of_id,
+                              float4* __restrict__ dst, int64_t n)
+{
+    const int64_t id = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= n) return;
+    dst[slot_of_id[id]] = make_float4(in[3 * id], in[3 * id + 1], in[3 * id + 2], 0.f);
+}
+
+void launch_scatter_vec(const float* in, const int32_t* slot_of_id, float4* dst, int64_t n, cudaStream_t s)
+{
+    if (n) k_scatter_vec<<<blocks_for(n), kThreads, 0, s>>>(in, slot_of_id, dst, n);
+}
+
 __global__ void k_gather_state(const float4* __restrict__ pos, const float4* __restrict__ vel,
                                const float4* __restrict__ hv, const float4* __restrict__ ov,
                                const int32_t* __restrict__ slot_of_id, float* x, float* v, float* h, float* o,

@@ -224,6 +224,15 @@ class SPHSolver:
         f = np.ascontiguousarray(first, np.int32).reshape(n)
         self._call("lsp_write_state", *(_ptr(a) for a in arrs), _ptr(f, POINTER(c_int32)), n)
 
+    def save_state(self, path: str, seed: int = 0):
+        """Writes the scene and its state to a file (lsp_save_state)."""
+        self._call("lsp_save_state", str(path).encode(), ctypes.c_uint64(seed))
+
+    def load_state(self, path: str):
+        """Replaces parameters, particles, colliders and grid box from a file (lsp_load_state)."""
+        self._call("lsp_load_state", str(path).encode())
+        self._colliders = []
+
     def neighbors(self):
         """Start-of-step neighbour lists of the last step: (offsets[n+1], caller ids)."""
         n = self.get_particle_count()
@@ -310,6 +319,17 @@ class PCISPHSolver(SPHSolver):
     def set_minimum_iteration_floor(self, n: int):
         """Extension: no convergence exit before n iterations (the reference has none)."""
         self.set_params(pci_min_iterations=int(n))
+
+
+def state_file_info(path: str) -> dict:
+    """Header of a state file (no device needed): params, particle count, colliders, seed."""
+    lib = abi.load_library()
+    p = abi.LspParams()
+    n = c_int64()
+    cols = c_int32()
+    seed = ctypes.c_uint64()
+    abi.check(lib, lib.lsp_state_file_info(str(path).encode(), byref(p), byref(n), byref(cols), byref(seed)))
+    return {"params": p, "n": n.value, "colliders": cols.value, "seed": seed.value}
 
 
 def from_scene(scene, device: int = -1) -> SPHSolver:
