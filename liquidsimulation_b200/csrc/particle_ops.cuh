@@ -172,10 +172,12 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
                              const V3 xj = v3(r.x);
                              V3 dir = xi - xj;
                              float d = mag(xj - xi);
-                             normal += dir * lookup(DW, TH, d, P) / r.rho;
-                             lap += lookup(D2W, TH, d, P) / r.rho;
-                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * lookup(VD2W, TH, d, P);
-                             if (kGrad) grad += dir * (lookup(DW, TH, d, P) * ((r.rho - rhoi) / r.rho));
+                             const TableIndex at(d, TH, P);
+                             const float w_dw = at(DW);
+                             normal += dir * w_dw / r.rho;
+                             lap += at(D2W) / r.rho;
+                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at(VD2W);
+                             if (kGrad) grad += dir * (w_dw * ((r.rho - rhoi) / r.rho));
                          });
     if (kGrad) b.gradrho[i] = P.mass * mag(grad);
     normal *= P.mass;
