@@ -171,7 +171,7 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
                          [&](int j, const Rec& r) {
                              const V3 xj = v3(r.x);
                              V3 dir = xi - xj;
-                             float d = mag(xj - xi);
+                             float d = mag(dir);   // equals |x_j - x_i| bit for bit
                              const TableIndex at(d, TH, P);
                              const float w_dw = at(DW);
                              normal += dir * w_dw / r.rho;
@@ -315,9 +315,11 @@ __device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuff
                          [&](int j) { return ppos[j]; },
                          [&](int j, float4 pj4) {
                              if (j == i) return;
-                             const V3 xj = v3(pj4);
-                             float d = mag(xj - xi);
-                             V3 dir = (xi - xj) / d;
+                             // |x_i - x_j| rounds exactly like the reference's |x_j - x_i|
+                             // (the squares are equal), so one difference serves both.
+                             const V3 dq = xi - v3(pj4);
+                             float d = mag(dq);
+                             V3 dir = dq / d;
                              pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
                          });
     pf *= -(P.mass * b.rho[i]);
