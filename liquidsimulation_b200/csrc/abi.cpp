@@ -11,24 +11,6 @@
 namespace {
 thread_local std::string g_last_error;
 
-template <typename F>
-int guard(F&& f)
-{
-    try {
-        f();
-        return LSP_OK;
-    } catch (const lsp::Error& e) {
-        g_last_error = e.what();
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        g_last_error = "host allocation failed";
-        return LSP_ERR_CAPACITY;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return LSP_ERR_INVALID;
-    }
-}
-
 lsp::Engine& E(lsp_solver* s)
 {
     if (!s || !s->e) throw lsp::Error(LSP_ERR_INVALID, "null solver handle");
@@ -80,7 +62,7 @@ const char* lsp_last_error(void) { return g_last_error.c_str(); }
 
 int lsp_device_info(int* sm_count, int* cc_major, int* cc_minor)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         int dev = 0, n = 0;
         if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) throw lsp::Error(LSP_ERR_NO_DEVICE, "no CUDA device");
         cudaGetDevice(&dev);
@@ -94,7 +76,7 @@ int lsp_device_info(int* sm_count, int* cc_major, int* cc_minor)
 
 int lsp_create(const lsp_params* params, int device, lsp_solver** out)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(params, "params");
         need(out, "out");
         *out = nullptr;
@@ -111,7 +93,7 @@ int lsp_create(const lsp_params* params, int device, lsp_solver** out)
 
 int lsp_destroy(lsp_solver* s)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         if (!s) return;
         delete s->e;
         delete s;
@@ -120,31 +102,31 @@ int lsp_destroy(lsp_solver* s)
 
 int lsp_set_params(lsp_solver* s, const lsp_params* p)
 {
-    return guard([&] { need(p, "params"); E(s).set_params(*p); });
+    return lsp::guard([&] { need(p, "params"); E(s).set_params(*p); });
 }
 int lsp_get_params(const lsp_solver* s, lsp_params* out)
 {
-    return guard([&] { need(out, "out"); *out = E(s).params(); });
+    return lsp::guard([&] { need(out, "out"); *out = E(s).params(); });
 }
 int lsp_particle_mass(const lsp_solver* s, float* m)
 {
-    return guard([&] { need(m, "mass"); *m = E(s).mass(); });
+    return lsp::guard([&] { need(m, "mass"); *m = E(s).mass(); });
 }
 int lsp_kernel_radius(const lsp_solver* s, float* h)
 {
-    return guard([&] { need(h, "h"); *h = E(s).kernel_radius(); });
+    return lsp::guard([&] { need(h, "h"); *h = E(s).kernel_radius(); });
 }
 int lsp_particle_count(const lsp_solver* s, int64_t* n)
 {
-    return guard([&] { need(n, "n"); *n = E(s).count(); });
+    return lsp::guard([&] { need(n, "n"); *n = E(s).count(); });
 }
 int lsp_pcisph_delta(const lsp_solver* s, float dt, float* delta)
 {
-    return guard([&] { need(delta, "delta"); *delta = E(s).delta(dt); });
+    return lsp::guard([&] { need(delta, "delta"); *delta = E(s).delta(dt); });
 }
 int lsp_kernel_tables(const lsp_solver* s, float* out, int capacity)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(out, "out");
         const auto& t = E(s).tables();
         const int n = 5 * lsp::kTableSize;
@@ -155,11 +137,11 @@ int lsp_kernel_tables(const lsp_solver* s, float* out, int capacity)
 
 int lsp_add_particles(lsp_solver* s, const float* xyz, const float* vel, int64_t n)
 {
-    return guard([&] { E(s).add_particles(xyz, vel, n); });
+    return lsp::guard([&] { E(s).add_particles(xyz, vel, n); });
 }
 int lsp_remove_particles(lsp_solver* s)
 {
-    return guard([&] { E(s).remove_particles(); });
+    return lsp::guard([&] { E(s).remove_particles(); });
 }
 
 static lsp::Collider box_of(const float c[3], const float h[3], int kind)
@@ -185,7 +167,7 @@ static lsp::Collider sphere_of(const float c[3], float r, int kind)
 
 int lsp_add_box(lsp_solver* s, const float center[3], const float half_extent[3], int kind)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         need(half_extent, "half_extent");
         E(s).add_collider(box_of(center, half_extent, kind));
@@ -193,18 +175,18 @@ int lsp_add_box(lsp_solver* s, const float center[3], const float half_extent[3]
 }
 int lsp_add_sphere(lsp_solver* s, const float center[3], float radius, int kind)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         E(s).add_collider(sphere_of(center, radius, kind));
     });
 }
 int lsp_remove_colliders(lsp_solver* s)
 {
-    return guard([&] { E(s).remove_colliders(); });
+    return lsp::guard([&] { E(s).remove_colliders(); });
 }
 int lsp_update_box(lsp_solver* s, int index, const float center[3], const float half_extent[3])
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         need(half_extent, "half_extent");
         E(s).update_collider(index, box_of(center, half_extent, LSP_OBSTACLE));
@@ -212,14 +194,14 @@ int lsp_update_box(lsp_solver* s, int index, const float center[3], const float 
 }
 int lsp_update_sphere(lsp_solver* s, int index, const float center[3], float radius)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         E(s).update_collider(index, sphere_of(center, radius, LSP_OBSTACLE));
     });
 }
 int lsp_set_domain(lsp_solver* s, const float lo[3], const float hi[3])
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(lo, "lo");
         need(hi, "hi");
         E(s).set_domain(lo, hi);
@@ -228,116 +210,116 @@ int lsp_set_domain(lsp_solver* s, const float lo[3], const float hi[3])
 
 int lsp_step(lsp_solver* s, float dt, lsp_step_stats* stats)
 {
-    return guard([&] { E(s).step(dt, stats); });
+    return lsp::guard([&] { E(s).step(dt, stats); });
 }
 int lsp_step_many(lsp_solver* s, float dt, int steps, lsp_step_stats* stats)
 {
-    return guard([&] { E(s).step_many(dt, steps, stats); });
+    return lsp::guard([&] { E(s).step_many(dt, steps, stats); });
 }
 int lsp_synchronize(lsp_solver* s)
 {
-    return guard([&] { E(s).synchronize(); });
+    return lsp::guard([&] { E(s).synchronize(); });
 }
 
 int lsp_read_particles(lsp_solver* s, float* xyz, float* vel, int64_t n)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         if (xyz) E(s).read_field(LSP_FIELD_POSITION, xyz, n);
         if (vel) E(s).read_field(LSP_FIELD_VELOCITY, vel, n);
     });
 }
 int lsp_read_field(lsp_solver* s, int field, float* out, int64_t n)
 {
-    return guard([&] { E(s).read_field(field, out, n); });
+    return lsp::guard([&] { E(s).read_field(field, out, n); });
 }
 int lsp_read_state(lsp_solver* s, float* x, float* v, float* half, float* old_half, int32_t* first, int64_t n)
 {
-    return guard([&] { E(s).read_state(x, v, half, old_half, first, n); });
+    return lsp::guard([&] { E(s).read_state(x, v, half, old_half, first, n); });
 }
 int lsp_write_state(lsp_solver* s, const float* x, const float* v, const float* half, const float* old_half,
                     const int32_t* first, int64_t n)
 {
-    return guard([&] { E(s).write_state(x, v, half, old_half, first, n); });
+    return lsp::guard([&] { E(s).write_state(x, v, half, old_half, first, n); });
 }
 int lsp_read_neighbors(lsp_solver* s, int64_t* offsets, int32_t* index, int64_t n, int64_t capacity)
 {
-    return guard([&] { E(s).read_neighbors(offsets, index, n, capacity); });
+    return lsp::guard([&] { E(s).read_neighbors(offsets, index, n, capacity); });
 }
 int lsp_grid_info(lsp_solver* s, int32_t dims[3], int32_t origin[3], int64_t* cells)
 {
-    return guard([&] { E(s).grid_info(dims, origin, cells); });
+    return lsp::guard([&] { E(s).grid_info(dims, origin, cells); });
 }
 int lsp_read_grid(lsp_solver* s, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start, int64_t cells_plus_one)
 {
-    return guard([&] { E(s).read_grid(keys, ids, n, cell_start, cells_plus_one); });
+    return lsp::guard([&] { E(s).read_grid(keys, ids, n, cell_start, cells_plus_one); });
 }
 
 int lsp_mlp_reset(lsp_solver* s, uint64_t seed)
 {
-    return guard([&] { E(s).mlp_reset(seed); });
+    return lsp::guard([&] { E(s).mlp_reset(seed); });
 }
 int lsp_mlp_set_weights(lsp_solver* s, const float* w, int n)
 {
-    return guard([&] { E(s).mlp_set(w, n); });
+    return lsp::guard([&] { E(s).mlp_set(w, n); });
 }
 int lsp_mlp_get_weights(lsp_solver* s, float* w, int n)
 {
-    return guard([&] { E(s).mlp_get(w, n); });
+    return lsp::guard([&] { E(s).mlp_get(w, n); });
 }
 int lsp_mlp_record(lsp_solver* s, int enable)
 {
-    return guard([&] { E(s).mlp_record(enable != 0); });
+    return lsp::guard([&] { E(s).mlp_record(enable != 0); });
 }
 int lsp_mlp_set_loss_asymmetry(lsp_solver* s, float over_weight)
 {
-    return guard([&] { E(s).mlp_set_loss_asymmetry(over_weight); });
+    return lsp::guard([&] { E(s).mlp_set_loss_asymmetry(over_weight); });
 }
 int lsp_mlp_train(lsp_solver* s, int iterations, int batch, float learning_rate, uint64_t seed, float* loss)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         float l = E(s).mlp_train(iterations, batch, learning_rate, seed);
         if (loss) *loss = l;
     });
 }
 int lsp_mlp_forward(lsp_solver* s, const float* features, int64_t n, float* out)
 {
-    return guard([&] { E(s).mlp_forward(features, n, out); });
+    return lsp::guard([&] { E(s).mlp_forward(features, n, out); });
 }
 int lsp_mlp_gradient(lsp_solver* s, const float* features, const float* targets, int64_t n, float* grad, float* loss)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         float l = E(s).mlp_gradient(features, targets, n, grad);
         if (loss) *loss = l;
     });
 }
 int lsp_read_features(lsp_solver* s, float* out, int64_t n)
 {
-    return guard([&] { E(s).read_features(out, n); });
+    return lsp::guard([&] { E(s).read_features(out, n); });
 }
 
 int lsp_timer_mark(lsp_solver* s, int slot)
 {
-    return guard([&] { E(s).timer_mark(slot); });
+    return lsp::guard([&] { E(s).timer_mark(slot); });
 }
 int lsp_timer_elapsed(lsp_solver* s, int slot_a, int slot_b, float* ms)
 {
-    return guard([&] { need(ms, "ms"); *ms = E(s).timer_elapsed(slot_a, slot_b); });
+    return lsp::guard([&] { need(ms, "ms"); *ms = E(s).timer_elapsed(slot_a, slot_b); });
 }
 int lsp_profile(lsp_solver* s, int enable)
 {
-    return guard([&] { E(s).profile(enable != 0); });
+    return lsp::guard([&] { E(s).profile(enable != 0); });
 }
 int lsp_profile_read(lsp_solver* s, double* ms, int64_t* launches, int capacity)
 {
-    return guard([&] { E(s).profile_read(ms, launches, capacity); });
+    return lsp::guard([&] { E(s).profile_read(ms, launches, capacity); });
 }
 int lsp_launch_count(const lsp_solver* s, int64_t* launches)
 {
-    return guard([&] { need(launches, "launches"); *launches = E(s).launch_count(); });
+    return lsp::guard([&] { need(launches, "launches"); *launches = E(s).launch_count(); });
 }
 int lsp_host_alloc(size_t bytes, void** out)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(out, "out");
         *out = nullptr;
         cudaError_t e = cudaMallocHost(out, bytes);
@@ -346,7 +328,7 @@ int lsp_host_alloc(size_t bytes, void** out)
 }
 int lsp_host_free(void* p)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         if (p) cudaFreeHost(p);
     });
 }

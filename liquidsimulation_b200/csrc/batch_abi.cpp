@@ -14,24 +14,6 @@ struct lsp_batch {
 
 namespace {
 
-template <typename F>
-int guard(F&& f)
-{
-    try {
-        f();
-        return LSP_OK;
-    } catch (const lsp::Error& e) {
-        lsp::set_last_error(e.what());
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        lsp::set_last_error("host allocation failed");
-        return LSP_ERR_CAPACITY;
-    } catch (const std::exception& e) {
-        lsp::set_last_error(e.what());
-        return LSP_ERR_INVALID;
-    }
-}
-
 lsp::BatchEngine& B(lsp_batch* b)
 {
     if (!b || !b->e) throw lsp::Error(LSP_ERR_INVALID, "null batch handle");
@@ -65,7 +47,7 @@ extern "C" {
 
 int lsp_batch_create(int device, lsp_batch** out)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(out, "out");
         *out = nullptr;
         lsp_batch* b = new lsp_batch{nullptr};
@@ -81,7 +63,7 @@ int lsp_batch_create(int device, lsp_batch** out)
 
 int lsp_batch_destroy(lsp_batch* b)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         if (!b) return;
         delete b->e;
         delete b;
@@ -91,7 +73,7 @@ int lsp_batch_destroy(lsp_batch* b)
 int lsp_batch_add_scene(lsp_batch* b, const lsp_params* params, const float* xyz, const float* vel, int64_t n,
                         const float* domain_lo, const float* domain_hi, int32_t* scene)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(params, "params");
         int s = B(b).add_scene(*params, xyz, vel, n, domain_lo, domain_hi);
         if (scene) *scene = s;
@@ -100,7 +82,7 @@ int lsp_batch_add_scene(lsp_batch* b, const lsp_params* params, const float* xyz
 
 int lsp_batch_add_box(lsp_batch* b, int32_t scene, const float center[3], const float half_extent[3], int kind)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         need(half_extent, "half_extent");
         B(b).add_collider(scene, collider(0, center, half_extent, 0.f, kind));
@@ -109,7 +91,7 @@ int lsp_batch_add_box(lsp_batch* b, int32_t scene, const float center[3], const 
 
 int lsp_batch_add_sphere(lsp_batch* b, int32_t scene, const float center[3], float radius, int kind)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         B(b).add_collider(scene, collider(1, center, nullptr, radius, kind));
     });
@@ -118,7 +100,7 @@ int lsp_batch_add_sphere(lsp_batch* b, int32_t scene, const float center[3], flo
 int lsp_batch_update_box(lsp_batch* b, int32_t scene, int32_t index, const float center[3],
                          const float half_extent[3])
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         need(half_extent, "half_extent");
         B(b).update_collider(scene, index, collider(0, center, half_extent, 0.f, LSP_OBSTACLE));
@@ -127,7 +109,7 @@ int lsp_batch_update_box(lsp_batch* b, int32_t scene, int32_t index, const float
 
 int lsp_batch_update_sphere(lsp_batch* b, int32_t scene, int32_t index, const float center[3], float radius)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(center, "center");
         B(b).update_collider(scene, index, collider(1, center, nullptr, radius, LSP_OBSTACLE));
     });
@@ -135,7 +117,7 @@ int lsp_batch_update_sphere(lsp_batch* b, int32_t scene, int32_t index, const fl
 
 int lsp_batch_info(const lsp_batch* b, int32_t* scenes, int64_t* particles)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         if (scenes) *scenes = B(b).scenes();
         if (particles) *particles = B(b).total();
     });
@@ -143,7 +125,7 @@ int lsp_batch_info(const lsp_batch* b, int32_t* scenes, int64_t* particles)
 
 int lsp_batch_scene_count(const lsp_batch* b, int32_t scene, int64_t* n)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(n, "n");
         *n = B(b).scene_count(scene);
     });
@@ -151,7 +133,7 @@ int lsp_batch_scene_count(const lsp_batch* b, int32_t scene, int64_t* n)
 
 int lsp_batch_particle_mass(const lsp_batch* b, int32_t scene, float* mass)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(mass, "mass");
         *mass = B(b).scene_mass(scene);
     });
@@ -159,96 +141,96 @@ int lsp_batch_particle_mass(const lsp_batch* b, int32_t scene, float* mass)
 
 int lsp_batch_step(lsp_batch* b, float dt, lsp_step_stats* stats)
 {
-    return guard([&] { B(b).step(dt, stats); });
+    return lsp::guard([&] { B(b).step(dt, stats); });
 }
 
 int lsp_batch_read_particles(lsp_batch* b, int32_t scene, float* xyz, float* vel, int64_t n)
 {
-    return guard([&] { B(b).read_particles(scene, xyz, vel, n); });
+    return lsp::guard([&] { B(b).read_particles(scene, xyz, vel, n); });
 }
 
 int lsp_batch_read_field(lsp_batch* b, int32_t scene, int field, float* out, int64_t n)
 {
-    return guard([&] { B(b).read_field(scene, field, out, n); });
+    return lsp::guard([&] { B(b).read_field(scene, field, out, n); });
 }
 
 int lsp_batch_read_neighbors(lsp_batch* b, int32_t scene, int64_t* offsets, int32_t* index, int64_t n,
                              int64_t capacity)
 {
-    return guard([&] { B(b).read_neighbors(scene, offsets, index, n, capacity); });
+    return lsp::guard([&] { B(b).read_neighbors(scene, offsets, index, n, capacity); });
 }
 
 int lsp_batch_grid_info(const lsp_batch* b, int32_t scene, int32_t dims[3], int32_t origin[3], int64_t* cells)
 {
-    return guard([&] { B(b).grid_info(scene, dims, origin, cells); });
+    return lsp::guard([&] { B(b).grid_info(scene, dims, origin, cells); });
 }
 
 int lsp_batch_read_grid(lsp_batch* b, int32_t scene, uint32_t* keys, int32_t* ids, int64_t n, uint32_t* cell_start,
                         int64_t cells_plus_one)
 {
-    return guard([&] { B(b).read_grid(scene, keys, ids, n, cell_start, cells_plus_one); });
+    return lsp::guard([&] { B(b).read_grid(scene, keys, ids, n, cell_start, cells_plus_one); });
 }
 
 int lsp_batch_read_state(lsp_batch* b, float* x, float* v, float* v_half, float* v_half_old, int32_t* first_step,
                          int64_t n)
 {
-    return guard([&] { B(b).read_state(x, v, v_half, v_half_old, first_step, n); });
+    return lsp::guard([&] { B(b).read_state(x, v, v_half, v_half_old, first_step, n); });
 }
 
 int lsp_batch_write_state(lsp_batch* b, const float* x, const float* v, const float* v_half,
                           const float* v_half_old, const int32_t* first_step, int64_t n)
 {
-    return guard([&] { B(b).write_state(x, v, v_half, v_half_old, first_step, n); });
+    return lsp::guard([&] { B(b).write_state(x, v, v_half, v_half_old, first_step, n); });
 }
 
 int lsp_batch_set_launch(lsp_batch* b, int use_graph, int threads, int loop_blocks)
 {
-    return guard([&] { B(b).set_launch(use_graph, threads, loop_blocks); });
+    return lsp::guard([&] { B(b).set_launch(use_graph, threads, loop_blocks); });
 }
 
 int lsp_batch_get_launch(const lsp_batch* b, int* use_graph, int* threads, int* loop_blocks, int* graph_active)
 {
-    return guard([&] { B(b).get_launch(use_graph, threads, loop_blocks, graph_active); });
+    return lsp::guard([&] { B(b).get_launch(use_graph, threads, loop_blocks, graph_active); });
 }
 
 int lsp_batch_autotune(lsp_batch* b, float dt, int repeats, lsp_batch_tuning* result, lsp_step_stats* stats)
 {
-    return guard([&] { B(b).autotune(dt, repeats, result, stats); });
+    return lsp::guard([&] { B(b).autotune(dt, repeats, result, stats); });
 }
 
 int lsp_batch_set_warm_start(lsp_batch* b, int mode)
 {
-    return guard([&] { B(b).set_warm_start(mode); });
+    return lsp::guard([&] { B(b).set_warm_start(mode); });
 }
 
 int lsp_batch_mlp_reset(lsp_batch* b, uint64_t seed)
 {
-    return guard([&] { B(b).mlp_reset(seed); });
+    return lsp::guard([&] { B(b).mlp_reset(seed); });
 }
 
 int lsp_batch_mlp_set_weights(lsp_batch* b, const float* w, int n)
 {
-    return guard([&] { B(b).mlp_set(w, n); });
+    return lsp::guard([&] { B(b).mlp_set(w, n); });
 }
 
 int lsp_batch_mlp_get_weights(lsp_batch* b, float* w, int n)
 {
-    return guard([&] { B(b).mlp_get(w, n); });
+    return lsp::guard([&] { B(b).mlp_get(w, n); });
 }
 
 int lsp_batch_mlp_record(lsp_batch* b, int on)
 {
-    return guard([&] { B(b).mlp_record(on != 0); });
+    return lsp::guard([&] { B(b).mlp_record(on != 0); });
 }
 
 int lsp_batch_mlp_set_loss_asymmetry(lsp_batch* b, float over_weight)
 {
-    return guard([&] { B(b).mlp_set_loss_asymmetry(over_weight); });
+    return lsp::guard([&] { B(b).mlp_set_loss_asymmetry(over_weight); });
 }
 
 int lsp_batch_mlp_train(lsp_batch* b, int iterations, int batch, float lr, uint64_t seed, float* loss)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         float l = B(b).mlp_train(iterations, batch, lr, seed);
         if (loss) *loss = l;
     });
@@ -256,17 +238,17 @@ int lsp_batch_mlp_train(lsp_batch* b, int iterations, int batch, float lr, uint6
 
 int lsp_batch_read_features(lsp_batch* b, int32_t scene, float* out, int64_t n)
 {
-    return guard([&] { B(b).read_features(scene, out, n); });
+    return lsp::guard([&] { B(b).read_features(scene, out, n); });
 }
 
 int lsp_batch_timer_mark(lsp_batch* b, int slot)
 {
-    return guard([&] { B(b).timer_mark(slot); });
+    return lsp::guard([&] { B(b).timer_mark(slot); });
 }
 
 int lsp_batch_timer_elapsed(lsp_batch* b, int slot_a, int slot_b, float* ms)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(ms, "ms");
         *ms = B(b).timer_elapsed(slot_a, slot_b);
     });
@@ -274,7 +256,7 @@ int lsp_batch_timer_elapsed(lsp_batch* b, int slot_a, int slot_b, float* ms)
 
 int lsp_batch_launch_count(const lsp_batch* b, int64_t* launches)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         need(launches, "launches");
         *launches = B(b).launch_count();
     });

@@ -93,24 +93,6 @@ Header read_header(FILE* f)
     return h;
 }
 
-template <typename F>
-int guard(F&& f)
-{
-    try {
-        f();
-        return LSP_OK;
-    } catch (const lsp::Error& e) {
-        lsp::set_last_error(e.what());
-        return e.code;
-    } catch (const std::bad_alloc&) {
-        lsp::set_last_error("host allocation failed");
-        return LSP_ERR_CAPACITY;
-    } catch (const std::exception& e) {
-        lsp::set_last_error(e.what());
-        return LSP_ERR_INVALID;
-    }
-}
-
 lsp::Engine& E(lsp_solver* s)
 {
     if (!s || !s->e) throw lsp::Error(LSP_ERR_INVALID, "null solver handle");
@@ -123,7 +105,7 @@ extern "C" {
 
 int lsp_save_state(lsp_solver* s, const char* path, uint64_t seed)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         lsp::Engine& e = E(s);
         const int64_t n = e.count();
         std::vector<float> x(3 * n), v(3 * n), hv(3 * n), ov(3 * n), hist;
@@ -174,7 +156,7 @@ int lsp_save_state(lsp_solver* s, const char* path, uint64_t seed)
 
 int lsp_load_state(lsp_solver* s, const char* path)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         lsp::Engine& e = E(s);
         File f = open_file(path, "rb");
         Header h = read_header(f.get());
@@ -228,7 +210,7 @@ int lsp_load_state(lsp_solver* s, const char* path)
 
 int lsp_state_file_info(const char* path, lsp_params* params, int64_t* n, int32_t* colliders, uint64_t* seed)
 {
-    return guard([&] {
+    return lsp::guard([&] {
         File f = open_file(path, "rb");
         Header h = read_header(f.get());
         if (params) *params = h.params;
