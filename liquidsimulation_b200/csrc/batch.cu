@@ -162,27 +162,23 @@ __global__ void __launch_bounds__(T) kb_pci_predict0(BatchArgs a, StepBuffers b)
     pci_predict_one(P, b, i, 0, b.ppos);
 }
 
-// Iteration 0's density with the warm-start features and, with mlp, the network's guess
-// (density_first_warp); p_scale = delta * 0.01 * rho0 of the item's scene. The scene's
-// maximum |error| goes to maxerr[scene * mstride].
+// Iteration 0's density with the warm-start features (density_first); p_scale = delta *
+// 0.01 * rho0 of the item's scene. The scene's maximum |error| goes to
+// maxerr[scene * mstride].
 template <int T>
 __global__ void __launch_bounds__(T) kb_density_first(BatchArgs a, StepBuffers b, BatchWarmArgs w)
 {
     __shared__ DevParams P;
     __shared__ float W[kTableSize], TH[kTableSize + 1];
-    __shared__ MlpPacked mw;
-    __shared__ uint32_t stage[T / 32][32 * 4];
     const BatchItem it = a.items[blockIdx.x];
     const float* tb = scene_tables(a, it.scene);
     stage_params(&P, a.sp, it.scene);
     stage_table(W, tb, T_W);
     stage_table(TH, tb, T_THRESH);
-    if (w.mlp) stage_mlp(&mw, w.mlp);
     __syncthreads();
     const int i = it.begin + (int)threadIdx.x;
     const float p_scale = P.delta * 0.01f * P.rho0;
-    const float e = density_first_warp(P, b, w.feat, b.hist, b.gradrho, w.mlp ? &mw : nullptr, p_scale, W, TH, i,
-                                       i < it.end, stage[threadIdx.x >> 5]);
+    const float e = density_first(P, b, w.feat, b.hist, b.gradrho, p_scale, W, TH, i, i < it.end);
     uint32_t m = __float_as_uint(e);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));

@@ -2,6 +2,7 @@
 // See batch_engine.h and batch_kernels.h.
 #include "batch_engine.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -384,11 +385,16 @@ int BatchEngine::enqueue_step(int c, int grid)
             // features and (warm start) the network's guess.
             BatchWarmArgs w{};
             w.feat = feat_.p;
-            w.mlp = warm_ == LSP_WARM_MLP ? mlp_.packed() : nullptr;
             w.maxerr = maxerr_.p;
             w.mstride = mstride_;
             launches += launch_batch_pci_predict0(a, b, stream_);
             launches += launch_batch_density_first(a, b, w, stream_);
+            if (warm_ == LSP_WARM_MLP) {
+                // The network's guess on the tensor cores, one block per item.
+                launch_batch_warm_guess_tc(mlp_.umma(), dparams_.p, items_.p, items_count_, b, feat_.p,
+                                           status_.p + S, stream_);
+                launches++;
+            }
         }
         BatchLoopArgs l{};
         l.ppos_alt = ppos_alt_.p;

@@ -52,11 +52,10 @@ int launch_batch_sph_pressure(const BatchArgs& a, const StepBuffers& b, cudaStre
 int launch_batch_integrate(const BatchArgs& a, const StepBuffers& b, bool add_pforce, cudaStream_t s);
 
 // Learned warm start of a batch: iteration 0's predict, then its density pass with the
-// features (b.hist, b.gradrho) and, with mlp, the network's guess; per-scene maximum
-// |error| to maxerr[scene * mstride]. Training targets p / p_scale per scene.
+// features (b.hist, b.gradrho); per-scene maximum |error| to maxerr[scene * mstride].
+// Training targets p / p_scale per scene. (The network's guess: mlp_tc.cuh.)
 struct BatchWarmArgs {
     float* feat;             // [n][8] features, written
-    const MlpPacked* mlp;    // null: features only (recording a plain step)
     uint32_t* maxerr;
     int mstride;
 };

@@ -1,6 +1,7 @@
 // Host engine: device memory, grid box, step sequencing. See engine.h.
 #include "engine.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -546,7 +547,6 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         w.feat = feat_.p;
         w.hist = phist_[cur_].p;
         w.gradrho = gradrho_.p;
-        w.mlp = warm ? mlp_.packed() : nullptr;
         w.p_scale = P.delta * 0.01f * P.rho0;
         last_p_scale_ = w.p_scale;
         features_valid_ = true;
@@ -557,7 +557,11 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         if (feats) {
             w.maxerr0 = maxerr_.p;
             timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, 0, stream_); return 1; });
-            timed(LSP_PROF_WARM_START, [&] { launch_pci_density_first(P, b, w, stream_); return 1; });
+            timed(LSP_PROF_WARM_START, [&] {
+                launch_pci_density_first(P, b, w, stream_);
+                if (warm) launch_warm_guess_tc(mlp_.umma(), P, b, feat_.p, stream_);
+                return warm ? 2 : 1;
+            });
         }
         bool ok = false;
         int grid = 0;
@@ -584,7 +588,11 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
     timed(LSP_PROF_PCI_PREDICT, [&] { launch_pci_predict(P, b, 0, stream_); return 1; });
     if (feats) {
         w.maxerr0 = &status_.p->max_err_bits;
-        timed(LSP_PROF_WARM_START, [&] { launch_pci_density_first(P, b, w, stream_); return 1; });
+        timed(LSP_PROF_WARM_START, [&] {
+            launch_pci_density_first(P, b, w, stream_);
+            if (warm) launch_warm_guess_tc(mlp_.umma(), P, b, feat_.p, stream_);
+            return warm ? 2 : 1;
+        });
     } else {
         timed(LSP_PROF_PCI_DENSITY, [&] { launch_pci_density(P, b, 0, stream_); return 1; });
     }

@@ -40,7 +40,6 @@ struct WarmArgs {
     float* feat;            // written when non-null (recording or warm start)
     const float4* hist;     // (p_{n-1}, p_{n-2}, p_{n-3}, -) per particle
     const float* gradrho;   // |grad rho| from the non-pressure pass
-    const MlpPacked* mlp;   // non-null: evaluate the MLP and seed p with its guess
     float p_scale;          // pressure of one correction at 1 % density error: delta * 0.01 * rho0
     uint32_t* maxerr0;      // max |error| of iteration 0 (float bits)
 };
@@ -95,12 +94,11 @@ void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // the maximum density error (the loop then restarts from zero pressure).
 bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
                      int first_done, int warm, cudaStream_t s, int* grid_used);
-// Iteration 0's density pass with the warm-start features (and, with w.mlp, the guess).
+// Iteration 0's density pass with the warm-start features.
 void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const WarmArgs& w, cudaStream_t s);
 
 // MLP (mlp.cu).
 void launch_mlp_pack(const float* master, MlpPacked* packed, cudaStream_t s);
-void launch_mlp_infer(const MlpPacked* packed, const float* feat, float* out, int n, cudaStream_t s);
 int mlp_grad_rows(int nb);
 void launch_mlp_grad(const MlpPacked* packed, const float* feat, const float* target, const int32_t* idx, int nb,
                      float over_weight, float* partial, float* loss_partial, cudaStream_t s);

@@ -1,7 +1,6 @@
 // Training and inference kernels of the warm-start MLP (see mlp.cuh for the layout).
 //
 //   k_mlp_pack   FP32 master parameters -> BF16 fragment-ordered weights + FP32 biases
-//   k_mlp_infer  features[n][8] -> outputs[n], one warp per 32 particles, 14 MMAs per tile
 //   k_mlp_grad   forward + backward on the tensor cores for a batch, MSE loss; the data
 //                gradients use the register-resident fragments, the weight gradients
 //                (reductions over particles) are MMAs whose operands are the transposed
@@ -66,26 +65,6 @@ __device__ __forceinline__ void load_packed(MlpPacked& s, const MlpPacked* g)
     const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s);
     for (int i = threadIdx.x; i < (int)(sizeof(MlpPacked) / 4); i += blockDim.x) dst[i] = src[i];
-}
-
-__global__ void __launch_bounds__(kMlpThreads) k_mlp_infer(const MlpPacked* __restrict__ wg,
-                                                          const float* __restrict__ feat, float* __restrict__ out,
-                                                          int n)
-{
-    __shared__ MlpPacked w;
-    __shared__ uint32_t stage[kMlpWarps][32 * 4];
-    load_packed(w, wg);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nwarps = gridDim.x * kMlpWarps;
-    for (int base = (blockIdx.x * kMlpWarps + warp) * 32; base < n; base += nwarps * 32) {
-        const int i = base + lane;
-        float f[kMlpIn];
-#pragma unroll
-        for (int c = 0; c < kMlpIn; c++) f[c] = i < n ? feat[(int64_t)i * kMlpIn + c] : 0.f;
-        float y = mlp_warp_eval(w, f, stage[warp]);
-        if (i < n) out[i] = y;
-    }
 }
 
 // Reads the bf16 element (row, col) of a row-major 16 x 32 tile stored as bf16x2 words.
@@ -342,12 +321,6 @@ void launch_mlp_pack(const float* master, MlpPacked* packed, cudaStream_t s)
     k_mlp_pack<<<1, 256, 0, s>>>(master, packed);
 }
 
-void launch_mlp_infer(const MlpPacked* packed, const float* feat, float* out, int n, cudaStream_t s)
-{
-    if (n <= 0) return;
-    int blocks = (n + kMlpThreads - 1) / kMlpThreads;
-    k_mlp_infer<<<blocks, kMlpThreads, 0, s>>>(packed, feat, out, n);
-}
 
 int mlp_grad_rows(int nb)
 {

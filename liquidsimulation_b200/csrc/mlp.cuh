@@ -1,5 +1,7 @@
 // Per-particle MLP of the learned PCISPH warm start: 8 features -> 32 -> 32 -> 1, SiLU,
-// BF16 operands on the tensor cores (mma.sync m16n8k16, FP32 accumulation).
+// BF16 operands on the tensor cores with FP32 accumulation. This header holds the training
+// side (warp-level mma.sync m16n8k16, whose fragments the backward pass reuses); inference
+// runs on tcgen05 (mlp_tc.cuh).
 //
 // A warp evaluates 32 particles as two 16-row tiles. The accumulator fragment of one
 // layer (rows g, g+8; columns 2q, 2q+1 of each 8-column tile; g = lane/4, q = lane%4)
@@ -100,34 +102,5 @@ __device__ __forceinline__ void mlp_tile_forward(const MlpPacked& w, const uint3
     y[1] = o[2];
 }
 
-// Evaluates the MLP for the 32 particles of a warp (one per lane). feat: this lane's 8
-// features; stage: 32 x 4 words of per-warp shared scratch. Returns this lane's output.
-// Every lane of the warp must call it (inactive lanes pass zeros).
-__device__ __forceinline__ float mlp_warp_eval(const MlpPacked& w, const float (&feat)[kMlpIn], uint32_t* stage)
-{
-    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-#pragma unroll
-    for (int p = 0; p < 4; p++) stage[lane * 4 + p] = pack_bf16(feat[2 * p], feat[2 * p + 1]);
-    __syncwarp();
-    float out[2][2];
-#pragma unroll
-    for (int m = 0; m < 2; m++) {
-        uint32_t a1[4] = {stage[(16 * m + g) * 4 + q], stage[(16 * m + g + 8) * 4 + q], 0u, 0u};
-        float z1[4][4], z2[4][4], y[2];
-        uint32_t h1[2][4], h2[2][4];
-        mlp_tile_forward<false>(w, a1, z1, z2, h1, h2, y);
-        out[m][0] = y[0];
-        out[m][1] = y[1];
-    }
-    __syncwarp();
-    // Row r of tile m lives in lane 4*(r%8) as y[r/8].
-    const int m = lane >> 4, r = lane & 15;
-    const int src = 4 * (r & 7);
-    float v0 = __shfl_sync(0xffffffffu, out[0][0], src);
-    float v1 = __shfl_sync(0xffffffffu, out[0][1], src);
-    float v2 = __shfl_sync(0xffffffffu, out[1][0], src);
-    float v3 = __shfl_sync(0xffffffffu, out[1][1], src);
-    return m == 0 ? (r < 8 ? v0 : v1) : (r < 8 ? v2 : v3);
-}
 
 }  // namespace lsp

@@ -8,6 +8,7 @@
 
 #include "lsp_kernels.h"
 #include "mlp.cuh"
+#include "mlp_tc.cuh"
 
 namespace lsp {
 
@@ -22,12 +23,16 @@ void MlpModel::init(cudaStream_t s)
     grad_.alloc(kMlpParams);
     loss_.alloc(1);
     packed_.alloc(sizeof(MlpPacked) / 4);
+    umma_.alloc(sizeof(MlpUmma) / 4);
+    err_.alloc(1);
+    CK(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), s_));
     reset(0);
 }
 
 void MlpModel::repack()
 {
     launch_mlp_pack(master_.p, reinterpret_cast<MlpPacked*>(packed_.p), s_);
+    launch_mlp_pack_umma(master_.p, reinterpret_cast<MlpUmma*>(umma_.p), s_);
     CK(cudaGetLastError());
 }
 
@@ -100,10 +105,16 @@ void MlpModel::forward(const float* feat, int64_t n, float* out)
     float* df = io_.p;
     float* dout = df + n * kMlpIn;
     CK(cudaMemcpyAsync(df, feat, n * kMlpIn * sizeof(float), cudaMemcpyHostToDevice, s_));
-    launch_mlp_infer(packed(), df, dout, (int)n, s_);
+    launch_mlp_forward_tc(umma(), df, dout, (int)n, err_.p, s_);
     CK(cudaGetLastError());
+    uint32_t err = 0;
     CK(cudaMemcpyAsync(out, dout, n * sizeof(float), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(&err, err_.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
+    if (err) {
+        CK(cudaMemsetAsync(err_.p, 0, sizeof(uint32_t), s_));
+        throw Error(LSP_ERR_TIMEOUT, "mlp_forward: a tensor-core accumulator wait gave up");
+    }
 }
 
 float MlpModel::gradient(const float* feat, const float* target, int64_t n, float* grad)

@@ -10,6 +10,7 @@
 namespace lsp {
 
 struct MlpPacked;
+struct MlpUmma;
 
 class MlpModel {
 public:
@@ -32,13 +33,15 @@ public:
     // Gradient of 1/(2n) sum (y - t)^2 at the current parameters (host in, host out).
     float gradient(const float* feat, const float* target, int64_t n, float* grad);
     const MlpPacked* packed() const { return reinterpret_cast<const MlpPacked*>(packed_.p); }
+    // The weights as tensor-core (tcgen05) operand images, for inference.
+    const MlpUmma* umma() const { return reinterpret_cast<const MlpUmma*>(umma_.p); }
 
 private:
     void repack();
     cudaStream_t s_ = nullptr;
     DevArray<float> master_, m1_, m2_, partial_, loss_part_, grad_, loss_, io_;
     DevArray<int32_t> idx_;
-    DevArray<uint32_t> packed_;
+    DevArray<uint32_t> packed_, umma_, err_;
     int step_ = 0;
     float over_weight_ = 1.f;
 };

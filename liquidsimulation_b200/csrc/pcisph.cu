@@ -81,22 +81,17 @@ void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 // ------------------------------------------------------------------ learned warm start
 
 // Iteration 0's density pass (PCISPHSolver.cpp:100-126 with p starting at 0) that also
-// computes the warm-start features and, with w.mlp, replaces the pressure of this first
-// correction by the network's guess (warm_ops.cuh). Without w.mlp its results are those of
-// the plain pass.
+// stores the warm-start features (warm_ops.cuh); its pressures are those of the plain pass
+// until the network's guess replaces them (mlp_tc.cu).
 __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, StepBuffers b, WarmArgs w)
 {
     __shared__ float W[kTableSize], TH[kTableSize + 1];
-    __shared__ MlpPacked mw;
-    __shared__ uint32_t stage[kThreads / 32][32 * 4];
     __shared__ float wmax[kThreads / 32];
     for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
     stage_thresholds(TH, b.tables);
-    if (w.mlp) stage_mlp(&mw, w.mlp);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float a = density_first_warp(P, b, w.feat, w.hist, w.gradrho, w.mlp ? &mw : nullptr, w.p_scale, W, TH, i,
-                                       i < P.n, stage[threadIdx.x >> 5]);
+    const float a = density_first(P, b, w.feat, w.hist, w.gradrho, w.p_scale, W, TH, i, i < P.n);
     uint32_t m = __float_as_uint(a);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));

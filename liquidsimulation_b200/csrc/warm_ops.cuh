@@ -1,6 +1,5 @@
-// Learned warm start, per particle: the features of iteration 0 and the density pass that
-// seeds the pressure with the network's guess. Shared by the single-scene kernel
-// (pcisph.cu) and the batched one (batch.cu).
+// Learned warm start, per particle: the features of iteration 0 and its density pass.
+// Shared by the single-scene kernel (pcisph.cu) and the batched one (batch.cu).
 #pragma once
 
 #include "lsp_kernels.h"
@@ -47,26 +46,16 @@ __device__ __forceinline__ void warm_features(const DevParams& P, const StepBuff
     f[7] = dist / (4.f * P.h);
 }
 
-// Copies the fragment-ordered network into shared memory (all threads of the block).
-__device__ __forceinline__ void stage_mlp(MlpPacked* sm, const MlpPacked* g)
-{
-    const uint32_t* src = reinterpret_cast<const uint32_t*>(g);
-    uint32_t* dst = reinterpret_cast<uint32_t*>(sm);
-    for (int t = threadIdx.x; t < (int)(sizeof(MlpPacked) / 4); t += blockDim.x) dst[t] = src[t];
-}
-
 // Iteration 0's density pass for particle i (PCISPHSolver.cpp:100-126 with p starting at 0)
-// with the warm-start features (stored when feat is non-null) and, with mw, the network's
-// pressure guess in place of the first correction. Every lane of the warp calls it (the
-// network runs on the warp's tensor cores); `valid` marks lanes with a particle. Returns
-// |error| (0 for NaN and for invalid lanes).
-__device__ __forceinline__ float density_first_warp(const DevParams& P, const StepBuffers& b, float* feat,
-                                                    const float4* hist, const float* gradrho, const MlpPacked* mw,
-                                                    float p_scale, const float* W, const float* TH, int i, bool valid,
-                                                    uint32_t* stage)
+// with the warm-start features (stored when feat is non-null); `valid` marks threads with a
+// particle. The network's guess, when used, replaces the stored first correction afterwards
+// (mlp_tc.cu). Returns |error| (0 for NaN and for invalid threads).
+__device__ __forceinline__ float density_first(const DevParams& P, const StepBuffers& b, float* feat,
+                                               const float4* hist, const float* gradrho, float p_scale,
+                                               const float* W, const float* TH, int i, bool valid)
 {
     float a = 0.f, pd = 0.f, p = 0.f;
-    float f[kMlpIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float f[kMlpIn];
     if (valid) {
         const V3 xi = v3(b.ppos[i]);
         const int cnt = __ldg(b.nbr_count + i);
@@ -89,13 +78,6 @@ __device__ __forceinline__ float density_first_warp(const DevParams& P, const St
         if (feat) {
 #pragma unroll
             for (int c = 0; c < kMlpIn; c++) feat[(int64_t)i * kMlpIn + c] = f[c];
-        }
-    }
-    if (mw) {
-        float y = mlp_warp_eval(*mw, f, stage);
-        if (valid) {
-            p = y * p_scale;
-            if (P.neg == 0.f && p < 0.f) p = 0.f;
         }
     }
     if (valid) {

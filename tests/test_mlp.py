@@ -1,5 +1,5 @@
 """Warm-start MLP: the FP64 oracle against finite differences (CPU), and the tensor-core
-forward / backward kernels against the oracle (GPU).
+forward (tcgen05) / backward (mma.sync) kernels against the oracle (GPU).
 
 Tolerances. Forward: |y_gpu - y_oracle| <= 2e-2 * (1 + |y|) per output (BF16 operands
 rounded at the same points, FP32 vs FP64 accumulation, occasional one-ulp BF16 flips of
@@ -64,6 +64,27 @@ def test_gpu_forward_matches_oracle():
     s._call("lsp_mlp_forward", x.ctypes.data_as(fp), 1000, out.ctypes.data_as(fp))
     ref, _ = M.forward(np.asarray(w, np.float32).astype(np.float64), x)
     assert np.all(np.abs(out - ref) <= 2e-2 * (1 + np.abs(ref))), np.max(np.abs(out - ref))
+    s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 127, 129, 100_003])
+def test_tensor_core_forward_tiles(n):
+    """The tcgen05 inference in 128-row tiles: a single row, ragged tails and more tiles than
+    resident blocks (grid-stride), against the oracle with a non-trivial output layer."""
+    s = _solver()
+    w = M.init(11)
+    w[M.OFF["W3"]:M.OFF["W3"] + 32] *= 10.0
+    w[M.OFF["b1"]:M.OFF["b1"] + 32] = np.linspace(-0.5, 0.5, 32)
+    _set(s, w)
+    x, _ = batch(n, 12)
+    out = np.empty(n, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    s._call("lsp_mlp_forward", x.ctypes.data_as(fp), n, out.ctypes.data_as(fp))
+    ref, _ = M.forward(np.asarray(w, np.float32).astype(np.float64), x)
+    err = np.abs(out - ref) / (1 + np.abs(ref))
+    assert np.all(err <= 2e-2), float(err.max())
+    assert np.median(err) < 2e-3
     s.close()
 
 
