@@ -51,7 +51,11 @@ __device__ __forceinline__ void mma16816(float (&d)[4], const uint32_t (&a)[4], 
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ float sigmoidf(float z) { return 1.f / (1.f + expf(-z)); }
+// The network's activations use the hardware approximations (__expf, __fdividef): the
+// library is compiled for IEEE-exact division and square roots (the physics needs them),
+// which the activations do not, and their error (a few ulp) is far below the BF16
+// rounding of every activation. For z < -87, __expf(-z) overflows and the quotient is 0.
+__device__ __forceinline__ float sigmoidf(float z) { return __fdividef(1.f, 1.f + __expf(-z)); }
 __device__ __forceinline__ float silu(float z) { return z * sigmoidf(z); }
 __device__ __forceinline__ float silu_grad(float z)
 {
