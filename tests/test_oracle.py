@@ -127,3 +127,28 @@ def test_scene_sizes_and_determinism():
     assert len(batch) == 64
     ns = [s.n for s in batch]
     assert min(ns) >= 1000 and max(ns) <= 70000
+
+
+@pytest.mark.parametrize("seed", range(16))
+def test_random_scenes_match_reference(oracle_mod, need_ref, seed):
+    """The restatement against the reference on the fuzz scenes (with the reference's
+    iteration rule: no minimum, and its first-step velocity wipe)."""
+    from fuzz_scenes import random_scene
+    scene, pci = random_scene(seed)
+    if pci:
+        scene.params.pci_min_iterations = 1
+        scene.params.keep_initial_velocity = 0
+    ref = oracle_mod.RefSolver(scene, capture_neighbors=True)
+    orc = oracle_mod.OracleSolver(scene)
+    for s in range(3):
+        it = ref.step(scene.dt)
+        st = orc.step(scene.dt)
+        if pci:
+            assert it == st.iterations, f"seed {seed} step {s}"
+        ro, ri = ref.neighbors()
+        oo, oi = orc.neighbors()
+        assert np.array_equal(ro, oo) and np.array_equal(ri, oi), f"seed {seed} step {s}: neighbour lists"
+        for f in FIELDS + (PCI_FIELDS if pci else []):
+            assert same_bits(ref.get(f), orc.get(f)), f"seed {seed} step {s} field {f}"
+    ref.close()
+    orc.close()
