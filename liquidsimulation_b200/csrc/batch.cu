@@ -90,16 +90,16 @@ template <int T>
 __global__ void __launch_bounds__(T) kb_density(BatchArgs a, StepBuffers b)
 {
     __shared__ DevParams P;
-    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
     const BatchItem it = a.items[blockIdx.x];
     const float* tb = scene_tables(a, it.scene);
     stage_params(&P, a.sp, it.scene);
     stage_table(W, tb, T_W);
-    stage_table(TH, tb, T_THRESH);
+    stage_table(TH2, tb, T_THRESH2);
     __syncthreads();
     const int i = it.begin + (int)threadIdx.x;
     if (i >= it.end) return;
-    density_one(P, b, W, TH, i);
+    density_one(P, b, W, TH2, i);
 }
 
 template <int T, bool kGrad>
@@ -169,16 +169,16 @@ template <int T>
 __global__ void __launch_bounds__(T) kb_density_first(BatchArgs a, StepBuffers b, BatchWarmArgs w)
 {
     __shared__ DevParams P;
-    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
     const BatchItem it = a.items[blockIdx.x];
     const float* tb = scene_tables(a, it.scene);
     stage_params(&P, a.sp, it.scene);
     stage_table(W, tb, T_W);
-    stage_table(TH, tb, T_THRESH);
+    stage_table(TH2, tb, T_THRESH2);
     __syncthreads();
     const int i = it.begin + (int)threadIdx.x;
     const float p_scale = P.delta * 0.01f * P.rho0;
-    const float e = density_first(P, b, w.feat, b.hist, b.gradrho, p_scale, W, TH, i, i < it.end);
+    const float e = density_first(P, b, w.feat, b.hist, b.gradrho, p_scale, W, TH2, i, i < it.end);
     uint32_t m = __float_as_uint(e);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
     int* preA = dyn + 2 * S;       // phase A item prefix (S + 1)
     int* preB = dyn + 3 * S + 1;   // phase B item prefix (S + 1)
     __shared__ DevParams P;
-    __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1], TH2[kTableSize + 1];
     __shared__ int staged;
     __shared__ int warp_sums[32];
     LoopSync* sy = reinterpret_cast<LoopSync*>(l.sync);
@@ -293,6 +293,7 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
         stage_table(W, tb, T_W);
         stage_table(SDW, tb, T_SPIKY_DW);
         stage_table(TH, tb, T_THRESH);
+        stage_table(TH2, tb, T_THRESH2);
         if (threadIdx.x == 0) staged = s;
         __syncthreads();
     };
@@ -392,7 +393,7 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
             const int k = st_k(w), kp = st_kp(w);
             const int i = P.base + j * T + (int)threadIdx.x;
             float m = 0.f;
-            if (i < P.base + P.n) m = pci_density_one(P, b, W, TH, i, k, pp(k));
+            if (i < P.base + P.n) m = pci_density_one(P, b, W, TH2, i, k, pp(k));
             // Max of non-negative floats: their bit patterns order like the values.
             uint32_t mb = __float_as_uint(m);
 #pragma unroll

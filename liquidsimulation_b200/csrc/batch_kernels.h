@@ -17,9 +17,9 @@
 namespace lsp {
 
 constexpr int kMaxBatchScenes = 4096;
-// Per-scene kernel tables: 5 tables of kTableSize, then the kTableSize + 1 slot thresholds,
-// padded to a multiple of 64 floats.
-constexpr int kSceneTableFloats = 5 * kTableSize + kTableSize + 1;
+// Per-scene kernel tables: the single-scene table block (5 tables of kTableSize, the slot
+// thresholds on d and on d^2), padded to a multiple of 64 floats.
+constexpr int kSceneTableFloats = kTableFloats;
 constexpr int kSceneTableStride = (kSceneTableFloats + 63) / 64 * 64;
 
 struct BatchItem {

@@ -32,8 +32,9 @@ void HostKernels::build(const lsp_params& p)
     float poly_d2 = (float)(-945.0 / (32.0 * pi * (double)r9));
     float spiky_d1 = (float)(-45.0 / (pi * (double)r6));
     float visc_d2 = (float)(45.0 / (pi * (double)r6));
-    // Five lookup tables, then the kTableSize + 1 slot thresholds of the device lookup.
-    tables.assign(6 * kTableSize + 1, 0.f);
+    // Five lookup tables, then the kTableSize + 1 slot thresholds of the device lookup on
+    // the distance, then the same thresholds on the squared distance.
+    tables.assign(kTableFloats, 0.f);
     for (int i = 0; i <= sub; i++) {
         float d = i * step;
         float t = r2 - d * d;
@@ -62,6 +63,28 @@ void HostKernels::build(const lsp_params& p)
         std::memcpy(&thr[k], &lo, 4);
     }
     thr[kTableSize] = std::numeric_limits<float>::infinity();
+    // thr2[k] = smallest float s >= 0 whose rounded square root reaches thr[k]: since the
+    // IEEE square root is monotone, sqrt(s) >= thr[k] exactly when s >= thr2[k], so a pass
+    // that needs the distance only for the table compares squared distances instead.
+    float* thr2 = tables.data() + kThresh2Offset;
+    auto sq_bound = [](float t) {
+        const float hi_s = 4.f * t * t + 1.f;
+        uint32_t lo = 0, hi;
+        std::memcpy(&hi, &hi_s, 4);
+        while (lo < hi) {
+            uint32_t mid = lo + (hi - lo) / 2;
+            float s;
+            std::memcpy(&s, &mid, 4);
+            if (std::sqrt(s) >= t) hi = mid; else lo = mid + 1;
+        }
+        float s;
+        std::memcpy(&s, &lo, 4);
+        return s;
+    };
+    thr2[0] = 0.f;
+    for (int k = 1; k <= sub; k++) thr2[k] = sq_bound(thr[k]);
+    thr2[kTableSize] = std::numeric_limits<float>::infinity();
+    cut2 = sq_bound(h);
     float stepSize = 1.6f * p.particle_radius;
     float sum = 0.f;
     for (int i = -3; i <= 3; i++)
@@ -407,6 +430,7 @@ DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt)
     P.gx = p.gravity[0]; P.gy = p.gravity[1]; P.gz = p.gravity[2];
     P.h = hk.h;
     P.h2 = hk.h * hk.h;
+    P.cut2 = hk.cut2;
     P.step = hk.step;
     P.inv_step = 1.f / hk.step;
     P.radius = p.particle_radius;

@@ -19,7 +19,8 @@ namespace lsp {
 // Reference-identical host arithmetic (compiled with -ffp-contract=off).
 struct HostKernels {
     float h = 0, step = 0, mass = 0;
-    std::vector<float> tables;   // 5 x 1001
+    float cut2 = 0;              // smallest float s with sqrt(s) >= h
+    std::vector<float> tables;   // 5 x 1001 tables, then the slot thresholds on d and on d^2
     void build(const lsp_params& p);
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;

@@ -15,6 +15,11 @@
 namespace lsp {
 
 constexpr int kTableSize = 1001;        // SPHKernel m_subdivision = 1000 (SPHKernel.cpp:4-7)
+// Kernel table block: 5 tables of kTableSize, the kTableSize + 1 slot thresholds on the
+// distance, then the kTableSize + 1 thresholds on the squared distance.
+constexpr int kThreshOffset = 5 * kTableSize;
+constexpr int kThresh2Offset = kThreshOffset + kTableSize + 1;
+constexpr int kTableFloats = kThresh2Offset + kTableSize + 1;
 constexpr int kMaxColliders = 64;
 constexpr int kMaxIterationsCap = 1024;
 
@@ -53,6 +58,7 @@ struct DevParams {
     float gx, gy, gz;
     float h;            // kernel radius = grid spacing
     float h2;           // h * h, the neighbour-test bound (SPHSpatialGrid.cpp:69)
+    float cut2;         // smallest float s with sqrt(s) >= h: the table cutoff on d^2
     float step;         // table division step h / 1000 (SPHKernel.cpp:134-137)
     float inv_step;     // 1 / step, rounded (only a first guess of the table slot)
     float radius;       // particle radius (collisions)
@@ -120,15 +126,38 @@ __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.
 // approximate quotient d * (1 / step), rounded to the nearest integer by the magic-number
 // addition (1.5 * 2^23), lands on that slot or the one above it (its relative error is a
 // few ulp and d / step < 1001), and one comparison with thr picks the right one. The
-// clamp keeps any input, NaN included, inside the table.
-__host__ __device__ __forceinline__ int table_slot(float d, float inv_step, const float* thr)
+// clamp keeps any input inside the table (slots 0..1000; NaN takes slot 1000, +inf too,
+// and the cutoff zeroes the latter).
+__host__ __device__ __forceinline__ int slot_guess(float d, float inv_step)
 {
     float r = d * inv_step + 12582912.f;
     int32_t bits;
     memcpy(&bits, &r, 4);
     int k = bits - 0x4B400000;
-    k = k < 1 ? 1 : (k > kTableSize ? kTableSize : k);
-    return (d >= thr[k]) ? k : k - 1;
+    return k < 1 ? 1 : (k > kTableSize - 1 ? kTableSize - 1 : k);
+}
+__host__ __device__ __forceinline__ int table_slot(float d, float inv_step, const float* thr)
+{
+    const int k = slot_guess(d, inv_step);
+    return !(d < thr[k]) ? k : k - 1;
+}
+
+// The same slot from the squared distance s = |dx|^2 for passes that need the distance only
+// for the table: the IEEE square root is monotone, so sqrt(s) >= thr[k] exactly when
+// s >= thr2[k] (thr2[k]: the smallest float whose rounded square root reaches thr[k], built
+// on the host by bisection). The first guess uses the approximate square root (relative
+// error near 2^-23, far inside the half-slot margin of the rounding guess); the comparison
+// is exact, so the slot is the one sqrt(s) would give, without the IEEE square root.
+__host__ __device__ __forceinline__ int table_slot_sq_from(float s, float d_guess, float inv_step, const float* thr2)
+{
+    const int k = slot_guess(d_guess, inv_step);
+    return !(s < thr2[k]) ? k : k - 1;
+}
+__device__ __forceinline__ int table_slot_sq(float s, float inv_step, const float* thr2)
+{
+    float d;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(d) : "f"(s));
+    return table_slot_sq_from(s, d, inv_step, thr2);
 }
 
 // The table read is unconditional (the slot is always inside the table) and the cutoff a
@@ -137,6 +166,13 @@ __device__ __forceinline__ float lookup(const float* tab, const float* thr, floa
 {
     const float w = tab[table_slot(d, P.inv_step, thr)];
     return (d >= P.h) ? 0.f : w;
+}
+// lookup(tab, thr, sqrt(s), P) bit for bit, from the squared distance (d >= h exactly when
+// s >= cut2).
+__device__ __forceinline__ float lookup_sq(const float* tab, const float* thr2, float s, const DevParams& P)
+{
+    const float w = tab[table_slot_sq(s, P.inv_step, thr2)];
+    return (s >= P.cut2) ? 0.f : w;
 }
 
 // One slot and cutoff for several tables read at the same distance (the compiler does not

@@ -9,13 +9,15 @@
 
 namespace lsp {
 
-enum { T_W = 0, T_DW = 1, T_D2W = 2, T_SPIKY_DW = 3, T_VISC_D2W = 4, T_THRESH = 5 };
+// T_THRESH: slot thresholds on the distance; T_THRESH2: on the squared distance.
+enum { T_W = 0, T_DW = 1, T_D2W = 2, T_SPIKY_DW = 3, T_VISC_D2W = 4, T_THRESH = 5, T_THRESH2 = 6 };
 
-// Copies table t (the threshold table has one entry more) into shared memory.
+// Copies table t (the threshold tables have one entry more) into shared memory.
 __device__ __forceinline__ void stage_table(float* sm, const float* g, int t)
 {
-    const int len = t == T_THRESH ? kTableSize + 1 : kTableSize;
-    for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[t * kTableSize + i];
+    const int len = t >= T_THRESH ? kTableSize + 1 : kTableSize;
+    const int off = t == T_THRESH2 ? kThresh2Offset : t * kTableSize;
+    for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[off + i];
 }
 
 // Cell key of a position inside the scene's grid box: the CPU grid's cell (int)(x / h)
@@ -130,14 +132,16 @@ __device__ __forceinline__ void record_neighbor_count(const DevParams& P, int c,
 }
 
 // SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
-__device__ __forceinline__ void density_one(const DevParams& P, const StepBuffers& b, const float* W, const float* TH,
-                                            int i)
+// The distance serves only the table, so the lookup takes the squared distance (TH2: the
+// thresholds on d^2; the same slot and value as the reference's sqrt-then-divide).
+__device__ __forceinline__ void density_one(const DevParams& P, const StepBuffers& b, const float* W,
+                                            const float* TH2, int i)
 {
     const V3 xi = v3(b.pos[i]);
     float sum = 0.f;
     for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return b.pos[j]; },
-                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+                         [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
     float rho = P.mass * sum;
     float pr = P.stiffness * (rho - P.rho0);
     if (pr < 0.f) pr *= P.neg;
@@ -274,15 +278,16 @@ __device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBu
 }
 
 // PCISPHSolver.cpp:100-126 for one particle; returns |error| (0 for NaN, which the
-// reference's std::max ignores).
+// reference's std::max ignores). Table lookups on the squared distance (TH2), as in
+// density_one.
 __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W,
-                                                 const float* TH, int i, int iteration, float4* ppos)
+                                                 const float* TH2, int i, int iteration, float4* ppos)
 {
     const V3 xi = v3(ppos[i]);
     float sum = 0.f;
     for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return ppos[j]; },
-                         [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+                         [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
     float pd = P.mass * sum;
     float er = pd - P.rho0;
     float pp = P.delta * er;

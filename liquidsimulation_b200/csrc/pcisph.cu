@@ -17,11 +17,6 @@ namespace lsp {
 
 constexpr int kThreads = 256;
 
-__device__ __forceinline__ void stage_thresholds(float* sm, const float* g)
-{
-    for (int t = threadIdx.x; t < kTableSize + 1; t += blockDim.x) sm[t] = g[T_THRESH * kTableSize + t];
-}
-
 __global__ void __launch_bounds__(kThreads) k_pci_predict(DevParams P, StepBuffers b, int iteration)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -32,13 +27,13 @@ __global__ void __launch_bounds__(kThreads) k_pci_predict(DevParams P, StepBuffe
 
 __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffers b, int iteration)
 {
-    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
     __shared__ float wmax[kThreads / 32];
-    for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
-    stage_thresholds(TH, b.tables);
+    stage_table(W, b.tables, T_W);
+    stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    float a = i < P.n ? pci_density_one(P, b, W, TH, i, iteration, b.ppos) : 0.f;
+    float a = i < P.n ? pci_density_one(P, b, W, TH2, i, iteration, b.ppos) : 0.f;
     // Max of non-negative floats: their bit patterns order like the values.
     uint32_t m = __float_as_uint(a);
 #pragma unroll
@@ -55,8 +50,8 @@ __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffe
 __global__ void __launch_bounds__(kThreads) k_pci_force(DevParams P, StepBuffers b)
 {
     __shared__ float SDW[kTableSize], TH[kTableSize + 1];
-    for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) SDW[t] = b.tables[T_SPIKY_DW * kTableSize + t];
-    stage_thresholds(TH, b.tables);
+    stage_table(SDW, b.tables, T_SPIKY_DW);
+    stage_table(TH, b.tables, T_THRESH);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
@@ -85,13 +80,13 @@ void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 // until the network's guess replaces them (mlp_tc.cu).
 __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, StepBuffers b, WarmArgs w)
 {
-    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
     __shared__ float wmax[kThreads / 32];
-    for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) W[t] = b.tables[T_W * kTableSize + t];
-    stage_thresholds(TH, b.tables);
+    stage_table(W, b.tables, T_W);
+    stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float a = density_first(P, b, w.feat, w.hist, w.gradrho, w.p_scale, W, TH, i, i < P.n);
+    const float a = density_first(P, b, w.feat, w.hist, w.gradrho, w.p_scale, W, TH2, i, i < P.n);
     uint32_t m = __float_as_uint(a);
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
@@ -135,13 +130,12 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 __global__ void __launch_bounds__(kThreads, 4) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt, LoopSync* sy,
                                                       uint32_t* maxerr, int first_done, int warm)
 {
-    __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1], TH2[kTableSize + 1];
     __shared__ float wmax[kThreads / 32];
-    for (int t = threadIdx.x; t < kTableSize; t += blockDim.x) {
-        W[t] = b.tables[T_W * kTableSize + t];
-        SDW[t] = b.tables[T_SPIKY_DW * kTableSize + t];
-    }
-    stage_thresholds(TH, b.tables);
+    stage_table(W, b.tables, T_W);
+    stage_table(SDW, b.tables, T_SPIKY_DW);
+    stage_table(TH, b.tables, T_THRESH);
+    stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
     float4* pp[2] = {b.ppos, ppos_alt};
     const int stride = gridDim.x * blockDim.x;
@@ -150,7 +144,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_pci_loop(DevParams P, StepBuffe
     // density(k) over all particles; the block maximum of |error| goes to maxerr[slot].
     auto density_pass = [&](int k, int slot) {
         float m = 0.f;
-        for (int i = tid; i < P.n; i += stride) m = fmaxf(m, pci_density_one(P, b, W, TH, i, k, pp[k & 1]));
+        for (int i = tid; i < P.n; i += stride) m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp[k & 1]));
         uint32_t mb = __float_as_uint(m);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, off));

@@ -16,13 +16,13 @@ constexpr int kThreads = 256;
 // SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
 __global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b)
 {
-    __shared__ float W[kTableSize], TH[kTableSize + 1];
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
     stage_table(W, b.tables, T_W);
-    stage_table(TH, b.tables, T_THRESH);
+    stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    density_one(P, b, W, TH, i);
+    density_one(P, b, W, TH2, i);
 }
 
 // SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248). The

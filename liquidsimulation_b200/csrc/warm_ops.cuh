@@ -52,7 +52,7 @@ __device__ __forceinline__ void warm_features(const DevParams& P, const StepBuff
 // (mlp_tc.cu). Returns |error| (0 for NaN and for invalid threads).
 __device__ __forceinline__ float density_first(const DevParams& P, const StepBuffers& b, float* feat,
                                                const float4* hist, const float* gradrho, float p_scale,
-                                               const float* W, const float* TH, int i, bool valid)
+                                               const float* W, const float* TH2, int i, bool valid)
 {
     float a = 0.f, pd = 0.f, p = 0.f;
     float f[kMlpIn];
@@ -61,7 +61,7 @@ __device__ __forceinline__ float density_first(const DevParams& P, const StepBuf
         const int cnt = __ldg(b.nbr_count + i);
         float sum = 0.f;
         for_each_neighbor<4>(b.nbr + i, P.nbr_stride, cnt, [&](int j) { return b.ppos[j]; },
-                             [&](int, float4 pj) { sum += lookup(W, TH, mag(v3(pj) - xi), P); });
+                             [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
         pd = P.mass * sum;
         float er = pd - P.rho0;
         float pp = P.delta * er;
