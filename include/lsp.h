@@ -314,7 +314,7 @@ int lsp_batch_read_state(lsp_batch* b, float* x, float* v, float* v_half, float*
                          int64_t n);
 int lsp_batch_write_state(lsp_batch* b, const float* x, const float* v, const float* v_half,
                           const float* v_half_old, const int32_t* first_step, int64_t n);
-/* Launch shape: use_graph (0/1), threads (128, 256 or 512 particles per block), loop_blocks
+/* Launch shape: use_graph (0/1), threads (128, 256, 512 or 1024 particles per block), loop_blocks
  * (blocks of the persistent kernel, 0 = all that fit). get also reports whether the step
  * currently runs as a captured graph. */
 int lsp_batch_set_launch(lsp_batch* b, int use_graph, int threads, int loop_blocks);

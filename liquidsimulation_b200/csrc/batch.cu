@@ -406,13 +406,17 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
 
 // ------------------------------------------------------------------ launchers
 
-bool batch_threads_supported(int threads) { return threads == 128 || threads == 256 || threads == 512; }
+bool batch_threads_supported(int threads)
+{
+    return threads == 128 || threads == 256 || threads == 512 || threads == 1024;
+}
 
 #define LSP_BATCH_DISPATCH(threads, BODY)                                                     \
     switch (threads) {                                                                         \
     case 128: { constexpr int T = 128; BODY; } break;                                         \
     case 256: { constexpr int T = 256; BODY; } break;                                         \
     case 512: { constexpr int T = 512; BODY; } break;                                         \
+    case 1024: { constexpr int T = 1024; BODY; } break;                                       \
     default: return 0;                                                                         \
     }
 
@@ -505,6 +509,7 @@ int batch_loop_max_blocks(int threads, int scenes)
     case 128: fn = loop_kernel<128>(); break;
     case 256: fn = loop_kernel<256>(); break;
     case 512: fn = loop_kernel<512>(); break;
+    case 1024: fn = loop_kernel<1024>(); break;
     default: return 0;
     }
     const size_t smem = loop_smem(scenes);
@@ -523,6 +528,7 @@ bool launch_batch_pci_loop(const BatchArgs& a, const StepBuffers& b, const Batch
     case 128: fn = loop_kernel<128>(); break;
     case 256: fn = loop_kernel<256>(); break;
     case 512: fn = loop_kernel<512>(); break;
+    case 1024: fn = loop_kernel<1024>(); break;
     default: return false;
     }
     BatchArgs ac = a;

@@ -520,7 +520,7 @@ void BatchEngine::step(float dt, lsp_step_stats* stats)
 
 void BatchEngine::set_launch(int use_graph, int threads, int loop_blocks)
 {
-    if (!batch_threads_supported(threads)) throw Error(LSP_ERR_INVALID, "threads must be 128, 256 or 512");
+    if (!batch_threads_supported(threads)) throw Error(LSP_ERR_INVALID, "threads must be 128, 256, 512 or 1024");
     if (loop_blocks < 0) throw Error(LSP_ERR_INVALID, "loop_blocks must be >= 0");
     use_graph_ = use_graph != 0;
     loop_blocks_ = loop_blocks;
@@ -557,7 +557,7 @@ void BatchEngine::autotune(float dt, int repeats, lsp_batch_tuning* out, lsp_ste
         float ms;
     };
     std::vector<Cand> cands;
-    for (int T : {128, 256, 512}) {
+    for (int T : {128, 256, 512, 1024}) {
         if (!pcisph_) {
             cands.push_back({T, 0, 0.f});
             continue;

@@ -125,13 +125,16 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 // The grid barrier spins with a bounded count: past the limit it raises kErrTimeout and
 // an abort word that makes every block leave; the host reports LSP_ERR_TIMEOUT.
 
-// 64 registers (four blocks per SM): measured about 10 % faster than the unconstrained
-// allocation (79 registers, three blocks per SM); three or five blocks are slower.
-__global__ void __launch_bounds__(kThreads, 4) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt, LoopSync* sy,
-                                                      uint32_t* maxerr, int first_done, int warm)
+// One 1024-thread block per SM at 64 registers: measured about 10 % faster than the
+// unconstrained allocation (79 registers, 768 threads per SM; 1280 threads per SM are
+// slower too), and one block of 1024 beats two of 512 by 3.5 % and four of 256 by 4 % (a
+// grid barrier with 148 arrivals, one table copy per SM).
+constexpr int kLoopThreads = 1024;
+__global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt,
+                                                             LoopSync* sy, uint32_t* maxerr, int first_done, int warm)
 {
     __shared__ float W[kTableSize], SDW[kTableSize], TH[kTableSize + 1], TH2[kTableSize + 1];
-    __shared__ float wmax[kThreads / 32];
+    __shared__ float wmax[kLoopThreads / 32];
     stage_table(W, b.tables, T_W);
     stage_table(SDW, b.tables, T_SPIKY_DW);
     stage_table(TH, b.tables, T_THRESH);
@@ -152,7 +155,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_pci_loop(DevParams P, StepBuffe
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t bm = 0;
-            for (int w = 0; w < kThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
+            for (int w = 0; w < kLoopThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
             if (bm) atomicMax(&maxerr[slot], bm);
         }
         __syncthreads();
@@ -219,19 +222,19 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
         cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
         int per = 0;
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kThreads, 0) == cudaSuccess)
+        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kLoopThreads, 0) == cudaSuccess)
             g_loop_blocks_per_sm = per;
         else
             g_loop_blocks_per_sm = 0;
     }
     if (g_loop_blocks_per_sm <= 0) return false;
-    int need = (int)((P.n + kThreads - 1) / kThreads);
+    int need = (int)((P.n + kLoopThreads - 1) / kLoopThreads);
     int grid = std::min(need, g_loop_blocks_per_sm * g_sm_count);
     DevParams Pc = P;
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;
     void* args[] = {&Pc, &bc, &ppos_alt, &sy, &maxerr, &first_done, &warm};
-    if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(kThreads), args, 0, s) != cudaSuccess)
+    if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(kLoopThreads), args, 0, s) != cudaSuccess)
         return false;
     if (grid_used) *grid_used = grid;
     return true;

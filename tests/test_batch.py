@@ -4,7 +4,7 @@ pins to the oracle bit for bit; one scene is also checked against the oracle dir
 
 Compared per step and scene: iteration counts and convergence, every per-particle field
 (0 ulp), neighbour lists, sorted keys, caller ids and the cell table. Launch shapes (graph
-or direct launches, 128/256/512 particles per block, persistent-kernel grid sizes) and the
+or direct launches, 128/256/512/1024 particles per block, persistent-kernel grid sizes) and the
 autotuner must not change a bit.
 """
 import numpy as np
@@ -106,6 +106,8 @@ def test_scene_matches_oracle_directly(oracle_mod):
     dict(use_graph=False, threads=256, loop_blocks=0),
     dict(use_graph=True, threads=128, loop_blocks=0),
     dict(use_graph=True, threads=512, loop_blocks=0),
+    dict(use_graph=True, threads=1024, loop_blocks=0),
+    dict(use_graph=False, threads=1024, loop_blocks=2),
     dict(use_graph=True, threads=256, loop_blocks=3),
 ])
 def test_launch_shape_does_not_change_bits(launch):
