@@ -190,6 +190,20 @@ struct TableIndex {
         return inside ? w : 0.f;
     }
 };
+// TableIndex of sqrt(s) from the squared distance s (thr2: the thresholds on d^2).
+struct TableIndexSq {
+    int k;
+    bool inside;
+    __device__ __forceinline__ TableIndexSq(float s, const float* thr2, const DevParams& P)
+        : k(table_slot_sq(s, P.inv_step, thr2)), inside(!(s >= P.cut2))
+    {
+    }
+    __device__ __forceinline__ float operator()(const float* tab) const
+    {
+        const float w = tab[k];
+        return inside ? w : 0.f;
+    }
+};
 
 // ----------------------------------------------------------------- collisions
 // StaticCollisionObject::resolveCollisionWithParticle (StaticCollisionObject.cpp:21-38).

@@ -152,10 +152,12 @@ __device__ __forceinline__ void density_one(const DevParams& P, const StepBuffer
 // SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248). The
 // reference walks the list up to three times (normal, colour Laplacian when the normal
 // exceeds the threshold, viscosity); each sum is independent, so one walk computes all
-// three with the same per-sum rounding. kGrad adds |grad rho|, a warm-start feature.
+// three with the same per-sum rounding. kGrad adds |grad rho|, a warm-start feature. The
+// distance serves only the tables (the normal sums the unnormalised difference), so the
+// slot comes from the squared distance (TH2).
 template <bool kGrad>
 __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float* DW,
-                                                const float* D2W, const float* VD2W, const float* TH, int i)
+                                                const float* D2W, const float* VD2W, const float* TH2, int i)
 {
     const V3 xi = v3(b.pos[i]);
     const V3 vi = v3(b.vel[i]);
@@ -175,8 +177,8 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
                          [&](int j, const Rec& r) {
                              const V3 xj = v3(r.x);
                              V3 dir = xi - xj;
-                             float d = mag(dir);   // equals |x_j - x_i| bit for bit
-                             const TableIndex at(d, TH, P);
+                             // |x_i - x_j|^2 equals |x_j - x_i|^2 bit for bit
+                             const TableIndexSq at(sqmag(dir), TH2, P);
                              const float w_dw = at(DW);
                              normal += dir * w_dw / r.rho;
                              lap += at(D2W) / r.rho;
