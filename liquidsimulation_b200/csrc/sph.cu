@@ -32,15 +32,12 @@ __global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b
 template <bool kGrad>
 __global__ void __launch_bounds__(kThreads) k_nonpressure(DevParams P, StepBuffers b)
 {
-    __shared__ float DW[kTableSize], D2W[kTableSize], VD2W[kTableSize], TH2[kTableSize + 1];
-    stage_table(TH2, b.tables, T_THRESH2);
-    stage_table(DW, b.tables, T_DW);
-    stage_table(D2W, b.tables, T_D2W);
-    stage_table(VD2W, b.tables, T_VISC_D2W);
+    __shared__ float4 NA[kTableSize], NB[kTableSize];
+    stage_nonpressure_slots(NA, NB, b.tables);
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
-    nonpressure_one<kGrad>(P, b, DW, D2W, VD2W, TH2, i);
+    nonpressure_one<kGrad>(P, b, NA, NB, i);
 }
 
 // SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
