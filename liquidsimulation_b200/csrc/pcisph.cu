@@ -208,28 +208,33 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     }
 }
 
-static int g_loop_blocks_per_sm = -1;
-static int g_sm_count = 0;
+// Per device: blocks of k_pci_loop per SM (0: no cooperative launch) and SM count.
+constexpr int kMaxDevices = 64;
+static int g_loop_blocks_per_sm[kMaxDevices];
+static int g_sm_count[kMaxDevices];
+static bool g_loop_ready[kMaxDevices];
 
 bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
                      int first_done, int warm, cudaStream_t s, int* grid_used)
 {
     if (grid_used) *grid_used = 0;
     if (P.n <= 0 || P.max_it <= 0) return false;
-    if (g_loop_blocks_per_sm < 0) {
-        int dev = 0, coop = 0;
-        cudaGetDevice(&dev);
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    if (!g_loop_ready[dev]) {
+        int coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev);
         int per = 0;
         if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kLoopThreads, 0) == cudaSuccess)
-            g_loop_blocks_per_sm = per;
+            g_loop_blocks_per_sm[dev] = per;
         else
-            g_loop_blocks_per_sm = 0;
+            g_loop_blocks_per_sm[dev] = 0;
+        g_loop_ready[dev] = true;
     }
-    if (g_loop_blocks_per_sm <= 0) return false;
+    if (g_loop_blocks_per_sm[dev] <= 0) return false;
     int need = (int)((P.n + kLoopThreads - 1) / kLoopThreads);
-    int grid = std::min(need, g_loop_blocks_per_sm * g_sm_count);
+    int grid = std::min(need, g_loop_blocks_per_sm[dev] * g_sm_count[dev]);
     DevParams Pc = P;
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;
