@@ -141,13 +141,30 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
     float4* pp[2] = {b.ppos, ppos_alt};
-    const int stride = gridDim.x * blockDim.x;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    // The particles of a pass: full rounds of one contiguous 1024-particle chunk per block,
+    // then the partial last round split evenly over all blocks (in whole warps), so that no
+    // SM runs a whole extra round while the others wait at the next grid barrier. Every pass
+    // maps particles to threads the same way (the bounds are recomputed per pass so that
+    // they hold no registers across the loop).
+    auto for_particles = [&](auto&& f) {
+        const int per_round = (int)gridDim.x * kLoopThreads;
+        const int full_end = (P.n / per_round) * per_round;
+        const int chunk = ((P.n - full_end + (int)gridDim.x - 1) / (int)gridDim.x + 31) & ~31;
+        const int j = full_end + (int)blockIdx.x * chunk + (int)threadIdx.x;
+        const int last = ((int)threadIdx.x < chunk && j < P.n) ? j : -1;
+        for (int i = tid;; i += per_round) {
+            const int q = i < full_end ? i : last;   // past the full rounds: the last-round particle
+            if (q < 0) break;
+            f(q);
+            if (i >= full_end) break;
+        }
+    };
 
     // density(k) over all particles; the block maximum of |error| goes to maxerr[slot].
     auto density_pass = [&](int k, int slot) {
         float m = 0.f;
-        for (int i = tid; i < P.n; i += stride) m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp[k & 1]));
+        for_particles([&](int i) { m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp[k & 1])); });
         uint32_t mb = __float_as_uint(m);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, off));
@@ -164,7 +181,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     int k = 0, kp = 0;
     bool conv = false, rejected = false;
     if (!first_done) {
-        for (int i = tid; i < P.n; i += stride) pci_predict_one(P, b, i, 0, pp[0]);
+        for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp[0]); });
         if (!grid_barrier(sy, b.status)) return;
         density_pass(0, 0);
         if (!grid_barrier(sy, b.status)) return;
@@ -176,7 +193,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
             rejected = true;
             k = 0;
             kp++;
-            for (int i = tid; i < P.n; i += stride) pci_predict_one(P, b, i, 0, pp[0]);
+            for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp[0]); });
             if (!grid_barrier(sy, b.status)) return;
             density_pass(0, kp);
             if (!grid_barrier(sy, b.status)) return;
@@ -188,10 +205,10 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
         // A learned guess is only checked at iteration 1, so a warm step cannot stop at 0.
         const bool unverified = warm && !rejected && k == 0;
         const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
-        for (int i = tid; i < P.n; i += stride) {
+        for_particles([&](int i) {
             pci_force_one(P, b, SDW, TH, i, pp[k & 1]);
             if (!done) pci_predict_one(P, b, i, k + 1, pp[(k + 1) & 1]);
-        }
+        });
         if (done) break;
         if (!grid_barrier(sy, b.status)) return;
         k++;
