@@ -468,7 +468,7 @@ bool BatchEngine::run_checked()
         if (!overflow) return true;
         if (attempt >= 3) return false;
         // The grid build left the pre-step buffers untouched: grow the lists and redo.
-        ensure_neighbors((int)need + (int)need / 4 + 8);
+        ensure_neighbors(grown_neighbor_capacity((int)need, nbr_cap_));
         upload_params(dt_);
     }
 }

@@ -662,6 +662,17 @@ int initial_neighbor_capacity(const lsp_params& p)
     return (int)std::min(4096.0, std::ceil(2.0 * est) + 16.0);
 }
 
+// At least 1.5x the count that overflowed and twice the old capacity, capped at the 4096
+// limit (unless the count itself is above it, which ensure_neighbors rejects). Every
+// regrowth frees and reallocates the whole list and redoes the step, and a large
+// cudaFree / cudaMalloc pair has been measured to take anywhere from 15 to 600 ms, so few
+// large steps beat many small ones.
+int grown_neighbor_capacity(int needed, int current)
+{
+    const int64_t c = std::max<int64_t>((int64_t)needed + needed / 2 + 8, 2 * (int64_t)current);
+    return (int)std::max<int64_t>(needed, std::min<int64_t>(c, 4096));
+}
+
 void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
 {
     (void)final_sync;
@@ -719,7 +730,7 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         if (profile_) collect_profile();
         if ((hstatus_->error_flags & kErrNeighborOverflow) && attempt < 3) {
             cur_ = 1 - cur_;   // the gather left the pre-step state untouched: redo the step
-            ensure_neighbors((int)hstatus_->max_neighbors + (int)hstatus_->max_neighbors / 4 + 8);
+            ensure_neighbors(grown_neighbor_capacity((int)hstatus_->max_neighbors, nbr_cap_));
             continue;
         }
         break;

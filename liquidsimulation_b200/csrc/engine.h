@@ -38,6 +38,8 @@ int64_t grid_from_box(const float lo[3], const float hi[3], float h, int32_t org
 DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt);
 // First neighbour-list capacity: twice the lattice estimate of the neighbour count.
 int initial_neighbor_capacity(const lsp_params& p);
+// Neighbour-list capacity after an overflow of `needed` entries with `current` allocated.
+int grown_neighbor_capacity(int needed, int current);
 
 class Engine {
 public:
