@@ -175,21 +175,6 @@ __device__ __forceinline__ float lookup_sq(const float* tab, const float* thr2, 
     return (s >= P.cut2) ? 0.f : w;
 }
 
-// One slot and cutoff for several tables read at the same distance (the compiler does not
-// merge separate lookups' slot arithmetic).
-struct TableIndex {
-    int k;
-    bool inside;
-    __device__ __forceinline__ TableIndex(float d, const float* thr, const DevParams& P)
-        : k(table_slot(d, P.inv_step, thr)), inside(!(d >= P.h))
-    {
-    }
-    __device__ __forceinline__ float operator()(const float* tab) const
-    {
-        const float w = tab[k];
-        return inside ? w : 0.f;
-    }
-};
 // The non-pressure pass reads three tables at one squared distance s. Its slot records
 // a[k] = {thr2[k], DW[k-1], DW[k], D2W[k-1]} and b[k] = {D2W[k], VD2W[k-1], VD2W[k], -} give
 // all three values with two 16-byte shared-memory reads once the first guess k is known,

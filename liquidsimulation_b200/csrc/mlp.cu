@@ -15,11 +15,6 @@ namespace lsp {
 constexpr int kMlpThreads = 256;
 constexpr int kMlpWarps = kMlpThreads / 32;
 
-__device__ __forceinline__ uint16_t bf16_bits(float x)
-{
-    __nv_bfloat16 b = __float2bfloat16_rn(x);
-    return *reinterpret_cast<uint16_t*>(&b);
-}
 __device__ __forceinline__ float bf16_to_float(uint16_t b)
 {
     return __uint_as_float(((uint32_t)b) << 16);
