@@ -50,6 +50,13 @@ extern "C" {
 /* ---- warm start of the PCISPH pressure ---- */
 #define LSP_WARM_ZERO      0   /* reference: p = 0, F_p = 0 (PCISPHSolver.cpp:58-62) */
 #define LSP_WARM_MLP       1   /* learned per-particle MLP guess, rejected if it raises the error */
+/* Zero start (bit-identical to LSP_WARM_ZERO) until a step needs more than
+ * warm_auto_iterations iterations or ends above eta; from the next step on, the learned
+ * guess of LSP_WARM_MLP. The learned guess costs iterations while plain PCISPH converges
+ * quickly and keeps a deep column converged once the plain loop starts running away, so
+ * this mode uses it only after the plain loop has shown trouble. It stays on until the
+ * parameters are set again (or a state file is loaded). No counterpart in the reference. */
+#define LSP_WARM_AUTO      2
 
 /* ---- PCISPH loop execution (results are identical) ---- */
 #define LSP_LOOP_PERSISTENT 0   /* one cooperative kernel, convergence decided on the device */
@@ -81,7 +88,8 @@ typedef struct lsp_params {
     int32_t strict_convergence;        /* 1: lsp_step returns LSP_ERR_NOT_CONVERGED at max iterations */
     int32_t keep_initial_velocity;     /* 1: skip the reference's first-step velocity wipe in PCISPH (Delta 5) */
     int32_t loop_mode;                 /* LSP_LOOP_*: how the PCISPH loop runs; default LSP_LOOP_PERSISTENT */
-    int32_t reserved[6];
+    int32_t warm_auto_iterations;      /* LSP_WARM_AUTO switch point (iterations); 0 = 12 */
+    int32_t reserved[5];
 } lsp_params;
 
 /* Per-step statistics, filled by lsp_step when non-NULL. */
@@ -92,7 +100,7 @@ typedef struct lsp_step_stats {
     int32_t max_neighbors;            /* largest neighbour count this step */
     int32_t escaped;                  /* particles outside the grid box (clamped into edge cells) */
     int32_t warm_start_used;          /* 1 if the warm-start guess was kept */
-    int32_t reserved;
+    int32_t warm_start_tried;         /* 1 if the step started from the learned guess (kept or not) */
 } lsp_step_stats;
 
 /* Fields for lsp_read_field. Vector fields are float[3*n], scalars float[n]. */

@@ -28,6 +28,7 @@ LSP_OBSTACLE = 0
 LSP_BOUNDARY = 1
 LSP_WARM_ZERO = 0
 LSP_WARM_MLP = 1
+LSP_WARM_AUTO = 2
 LSP_LOOP_PERSISTENT = 0
 LSP_LOOP_HOST = 1
 
@@ -80,7 +81,8 @@ class LspParams(ctypes.Structure):
         ("strict_convergence", c_int32),
         ("keep_initial_velocity", c_int32),
         ("loop_mode", c_int32),
-        ("reserved", c_int32 * 6),
+        ("warm_auto_iterations", c_int32),
+        ("reserved", c_int32 * 5),
     ]
 
 
@@ -92,7 +94,7 @@ class LspStepStats(ctypes.Structure):
         ("max_neighbors", c_int32),
         ("escaped", c_int32),
         ("warm_start_used", c_int32),
-        ("reserved", c_int32),
+        ("warm_start_tried", c_int32),
     ]
 
 

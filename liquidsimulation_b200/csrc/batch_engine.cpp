@@ -490,6 +490,7 @@ void BatchEngine::finish_step(lsp_step_stats* stats)
             local.converged = st.converged;
             local.max_density_error_ratio = (double)me / (double)sc_[s].prm.rest_density;
             local.warm_start_used = st.warm_used;
+            local.warm_start_tried = warm_ == LSP_WARM_MLP ? 1 : 0;
             sc_[s].last_k = st.last_k;
             if (sc_[s].prm.strict_convergence && !st.converged) not_converged = true;
         } else {
@@ -791,7 +792,8 @@ void BatchEngine::ensure_warm_buffers()
 
 void BatchEngine::set_warm_start(int mode)
 {
-    if (mode != LSP_WARM_ZERO && mode != LSP_WARM_MLP) throw Error(LSP_ERR_INVALID, "unknown warm_start");
+    if (mode != LSP_WARM_ZERO && mode != LSP_WARM_MLP)
+        throw Error(LSP_ERR_INVALID, "a batch's warm start is LSP_WARM_ZERO or LSP_WARM_MLP");
     if (mode == LSP_WARM_MLP && !sc_.empty() && !pcisph_)
         throw Error(LSP_ERR_INVALID, "the learned warm start needs PCISPH scenes");
     warm_ = mode;

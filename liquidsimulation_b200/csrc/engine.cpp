@@ -140,7 +140,9 @@ void validate_params(const lsp_params& p)
     if (p.solver != LSP_SOLVER_SPH && p.solver != LSP_SOLVER_PCISPH) bad("solver must be LSP_SOLVER_SPH or LSP_SOLVER_PCISPH");
     if (p.pci_max_iterations < 0 || p.pci_max_iterations > kMaxIterationsCap) bad("pci_max_iterations out of range [0, 1024]");
     if (p.pci_min_iterations < 0) bad("pci_min_iterations must be >= 0");
-    if (p.warm_start != LSP_WARM_ZERO && p.warm_start != LSP_WARM_MLP) bad("unknown warm_start");
+    if (p.warm_start != LSP_WARM_ZERO && p.warm_start != LSP_WARM_MLP && p.warm_start != LSP_WARM_AUTO)
+        bad("unknown warm_start");
+    if (p.warm_auto_iterations < 0) bad("warm_auto_iterations must be >= 0");
     if (p.loop_mode != LSP_LOOP_PERSISTENT && p.loop_mode != LSP_LOOP_HOST) bad("unknown loop_mode");
 }
 
@@ -195,6 +197,7 @@ void Engine::set_params(const lsp_params& p)
     bool geometry = p.particle_radius != prm_.particle_radius || p.kernel_radius_factor != prm_.kernel_radius_factor;
     prm_ = p;
     derive();
+    auto_on_ = false;            // LSP_WARM_AUTO starts from the zero start again
     if (geometry) nbr_cap_ = 0;  // re-estimate the list capacity for the new h
 }
 
@@ -553,7 +556,20 @@ float Engine::timer_elapsed(int a, int b)
 
 bool Engine::features_on() const
 {
-    return prm_.solver == LSP_SOLVER_PCISPH && (record_ || prm_.warm_start == LSP_WARM_MLP);
+    return prm_.solver == LSP_SOLVER_PCISPH && (record_ || warm_on());
+}
+
+bool Engine::history_on() const
+{
+    // LSP_WARM_AUTO keeps the pressure history (the features' three previous pressures)
+    // from the first step, so that the learned guess has it when the mode switches it on;
+    // the features themselves are computed only once the guess is on.
+    return prm_.solver == LSP_SOLVER_PCISPH && (record_ || prm_.warm_start != LSP_WARM_ZERO);
+}
+
+bool Engine::warm_on() const
+{
+    return prm_.warm_start == LSP_WARM_MLP || (prm_.warm_start == LSP_WARM_AUTO && auto_on_);
 }
 
 bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st)
@@ -565,7 +581,7 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         return false;
     }
     const bool feats = features_on();
-    const bool warm = prm_.warm_start == LSP_WARM_MLP;
+    const bool warm = warm_on();
     WarmArgs w{};
     if (feats) {
         w.feat = feat_.p;
@@ -650,6 +666,7 @@ bool Engine::pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stat
         st->converged = conv ? 1 : 0;
         st->max_density_error_ratio = (double)e / (double)prm_.rest_density;
         st->warm_start_used = (warm && !rejected) ? 1 : 0;
+        st->warm_start_tried = warm ? 1 : 0;
     }
     return false;
 }
@@ -692,7 +709,7 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         tables_dirty_ = false;
     }
     if (!dcols_.p) upload_colliders();
-    if (features_on()) ensure_warm_buffers();
+    if (history_on()) ensure_warm_buffers();
     if (nbr_cap_ == 0 || nbr_stride_ < cap_) ensure_neighbors(nbr_cap_ ? nbr_cap_ : initial_neighbor_capacity(prm_));
     lsp_step_stats local{};
     bool device_loop = false;
@@ -743,11 +760,17 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         local.converged = hstatus_->converged;
         local.max_density_error_ratio = (double)me / (double)prm_.rest_density;
         local.warm_start_used = hstatus_->warm_used;
+        local.warm_start_tried = warm_on() ? 1 : 0;
         ppos_final_ = (hstatus_->last_k & 1) ? ppos_alt_.p : ppos_.p;
     }
     local.max_neighbors = (int32_t)hstatus_->max_neighbors;
     local.escaped = (int32_t)hstatus_->escaped;
     if (st) *st = local;
+    // LSP_WARM_AUTO: a zero-start step that needed more iterations than the switch point, or
+    // missed eta, turns the learned guess on from the next step.
+    if (prm_.warm_start == LSP_WARM_AUTO && !auto_on_ && prm_.solver == LSP_SOLVER_PCISPH &&
+        (local.iterations > (prm_.warm_auto_iterations > 0 ? prm_.warm_auto_iterations : 12) || !local.converged))
+        auto_on_ = true;
     if (hstatus_->escaped && domain_from_particles_) grid_valid_ = false;
     if (hstatus_->error_flags & kErrTimeout)
         throw Error(LSP_ERR_TIMEOUT, "a grid barrier of the persistent PCISPH loop gave up");

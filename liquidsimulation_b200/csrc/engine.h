@@ -177,8 +177,11 @@ private:
 
     // Learned warm start state.
     bool features_on() const;
+    bool warm_on() const;      // this step starts from the learned guess
+    bool history_on() const;   // the pressure history is kept
     void ensure_warm_buffers();
     bool record_ = false, features_valid_ = false;
+    bool auto_on_ = false;  // LSP_WARM_AUTO has switched the learned guess on
     float last_p_scale_ = 1.f;
     DevArray<float4> phist_[2];   // pressure history (p_{n-1}, p_{n-2}, p_{n-3})
     DevArray<float> feat_, gradrho_, tgt_;

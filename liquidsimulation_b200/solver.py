@@ -73,6 +73,7 @@ class SPHSolver:
         return p
 
     def set_params(self, **fields):
+        """Changes parameters by field name; on an error the solver keeps the previous ones."""
         p = self.params
         for k, v in fields.items():
             if k == "gravity":

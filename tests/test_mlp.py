@@ -217,3 +217,54 @@ def test_trained_warm_start_converges():
     assert np.array_equal(a.mlp_get_weights(), b.mlp_get_weights())
     for s in solvers:
         s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("loop_mode", [abi.LSP_LOOP_PERSISTENT, abi.LSP_LOOP_HOST])
+def test_auto_warm_start_is_plain_until_its_switch_point(loop_mode):
+    """LSP_WARM_AUTO with a switch point the scene never reaches runs the zero start: the
+    same bits and iteration counts as LSP_WARM_ZERO, and no step tries the guess."""
+    from liquidsimulation_b200.solver import from_scene
+    sc = _warm_scene(loop_mode=loop_mode, pci_min_iterations=3)
+    plain = from_scene(sc)
+    auto = from_scene(sc)
+    auto.mlp_set_weights(M.init(2).astype(np.float32))
+    auto.set_params(warm_start=abi.LSP_WARM_AUTO, warm_auto_iterations=1000)
+    for step in range(4):
+        sp, sa = plain.update(sc.dt), auto.update(sc.dt)
+        assert sa.iterations == sp.iterations and sa.warm_start_tried == 0 and sa.warm_start_used == 0
+        for f in (abi.FIELD_POSITION, abi.FIELD_VELOCITY, abi.FIELD_DENSITY, abi.FIELD_PRESSURE):
+            assert np.array_equal(plain.read(f).view(np.uint32), auto.read(f).view(np.uint32)), (step, f)
+    plain.close()
+    auto.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("loop_mode", [abi.LSP_LOOP_PERSISTENT, abi.LSP_LOOP_HOST])
+def test_auto_warm_start_switches_after_a_slow_step(loop_mode):
+    """A step above the switch point turns the learned guess on from the next step: the run
+    matches a solver that records features on the first step and is set to LSP_WARM_MLP
+    after it, bit for bit, and stays on."""
+    from liquidsimulation_b200.solver import from_scene
+    sc = _warm_scene(loop_mode=loop_mode, pci_min_iterations=3)
+    w = M.init(4).astype(np.float32)
+    auto = from_scene(sc)
+    auto.mlp_set_weights(w)
+    auto.set_params(warm_start=abi.LSP_WARM_AUTO, warm_auto_iterations=2)
+    ref = from_scene(sc)
+    ref.mlp_set_weights(w)
+    ref.mlp_record(True)
+    for step in range(4):
+        sa, sr = auto.update(sc.dt), ref.update(sc.dt)
+        assert sa.warm_start_tried == (1 if step > 0 else 0)
+        assert (sa.iterations, sa.warm_start_used) == (sr.iterations, sr.warm_start_used)
+        for f in (abi.FIELD_POSITION, abi.FIELD_VELOCITY, abi.FIELD_DENSITY, abi.FIELD_PRESSURE):
+            assert np.array_equal(ref.read(f).view(np.uint32), auto.read(f).view(np.uint32)), (step, f)
+        if step == 0:
+            ref.set_warm_start(abi.LSP_WARM_MLP)
+    with pytest.raises(abi.LspError):
+        auto.set_params(warm_start=3)
+    with pytest.raises(abi.LspError):
+        auto.set_params(warm_auto_iterations=-1)
+    auto.close()
+    ref.close()
