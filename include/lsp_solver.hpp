@@ -153,6 +153,18 @@ public:
     float getMaxDensityErrorRatio() const { return params().pci_eta; }
     void setMinIterations(int v) { edit([&](lsp_params& p) { p.pci_max_iterations = v; }); }
     void setMaxDensityErrorRatio(float v) { edit([&](lsp_params& p) { p.pci_eta = v; }); }
+    // Extension (no counterpart in the reference): the initial pressure of the loop,
+    // LSP_WARM_ZERO (the reference), LSP_WARM_MLP (the learned guess, lsp_mlp_* in lsp.h) or
+    // LSP_WARM_AUTO (zero start until a step needs more than `autoIterations` iterations or
+    // misses eta, the learned guess after that; 0 = 12).
+    void setWarmStart(int mode, int autoIterations = 0)
+    {
+        edit([&](lsp_params& p) {
+            p.warm_start = mode;
+            p.warm_auto_iterations = autoIterations;
+        });
+    }
+    int getWarmStart() const { return params().warm_start; }
 };
 
 // Many independent scenes stepped together (lsp_batch_* in lsp.h): what an application
