@@ -79,17 +79,23 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
     }
     const int cap = P.nbr_cap;
     const int64_t stride = P.nbr_stride;
+    int32_t* out = nbr + i;
     int c = 0;
     if (lo[2] <= hi[2]) {
         for (int cx = lo[0]; cx <= hi[0]; cx++) {
             for (int cy = lo[1]; cy <= hi[1]; cy++) {
                 uint32_t row = P.cell_base + ((uint32_t)cx * (uint32_t)P.ny + (uint32_t)cy) * (uint32_t)P.nz;
-                uint32_t beg = cell_start[row + lo[2]];
-                uint32_t end = cell_start[row + hi[2] + 1];
-                for (uint32_t q = beg; q < end; q++) {
-                    V3 dq = xi - v3(pos[q]);
+                const uint32_t beg = cell_start[row + lo[2]];
+                const uint32_t end = cell_start[row + hi[2] + 1];
+                const float4* pe = pos + end;
+                int32_t q = (int32_t)beg;
+                for (const float4* pq = pos + beg; pq < pe; pq++, q++) {
+                    const V3 dq = xi - v3(*pq);
                     if (sqmag(dq) <= P.h2) {
-                        if (c < cap) nbr[(int64_t)c * stride + i] = (int32_t)q;
+                        if (c < cap) {
+                            *out = q;
+                            out += stride;
+                        }
                         c++;
                     }
                 }
