@@ -88,7 +88,7 @@ typedef struct lsp_params {
     int32_t strict_convergence;        /* 1: lsp_step returns LSP_ERR_NOT_CONVERGED at max iterations */
     int32_t keep_initial_velocity;     /* 1: skip the reference's first-step velocity wipe in PCISPH (Delta 5) */
     int32_t loop_mode;                 /* LSP_LOOP_*: how the PCISPH loop runs; default LSP_LOOP_PERSISTENT */
-    int32_t warm_auto_iterations;      /* LSP_WARM_AUTO switch point (iterations); 0 = 12 */
+    int32_t warm_auto_iterations;      /* LSP_WARM_AUTO switch point (iterations); 0 = max(12, pci_max_iterations / 2) */
     int32_t reserved[5];
 } lsp_params;
 
@@ -332,9 +332,10 @@ int lsp_batch_get_launch(const lsp_batch* b, int* use_graph, int* threads, int* 
  * per candidate, keeps the fastest shape, and leaves the batch advanced by exactly that one
  * step (results do not depend on the shape). result and stats may be NULL. */
 int lsp_batch_autotune(lsp_batch* b, float dt, int repeats, lsp_batch_tuning* result, lsp_step_stats* stats);
-/* Learned warm start for every scene of a PCISPH batch (LSP_WARM_ZERO or LSP_WARM_MLP):
- * one network for the batch, features normalised per scene, the guess checked and rejected
- * per scene exactly as lsp_step does. The lsp_mlp_* counterparts below act on the batch's
+/* Learned warm start for the scenes of a PCISPH batch (LSP_WARM_ZERO, LSP_WARM_MLP or
+ * LSP_WARM_AUTO; AUTO switches each scene on by itself, at that scene's
+ * warm_auto_iterations): one network for the batch, features normalised per scene, the
+ * guess checked and rejected per scene exactly as lsp_step does. The lsp_mlp_* counterparts below act on the batch's
  * network; train uses the features and final pressures of the last recorded step of all
  * scenes. No counterpart in the reference. */
 int lsp_batch_set_warm_start(lsp_batch* b, int mode);

@@ -156,7 +156,7 @@ public:
     // Extension (no counterpart in the reference): the initial pressure of the loop,
     // LSP_WARM_ZERO (the reference), LSP_WARM_MLP (the learned guess, lsp_mlp_* in lsp.h) or
     // LSP_WARM_AUTO (zero start until a step needs more than `autoIterations` iterations or
-    // misses eta, the learned guess after that; 0 = 12).
+    // misses eta, the learned guess after that; 0 = max(12, max iterations / 2)).
     void setWarmStart(int mode, int autoIterations = 0)
     {
         edit([&](lsp_params& p) {

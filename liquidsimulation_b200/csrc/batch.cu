@@ -325,7 +325,8 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
                     const DevParams* ps = a.sp + s;
                     const uint32_t* me_s = l.maxerr + (size_t)s * l.mstride;
                     const float me = __uint_as_float(ld_volatile(me_s + kp));
-                    if (l.warm && !rej && k == 1 && me > __uint_as_float(ld_volatile(me_s + kp - 1))) {
+                    const bool warm = l.warm && (!l.warm_scene || l.warm_scene[s]);
+                    if (warm && !rej && k == 1 && me > __uint_as_float(ld_volatile(me_s + kp - 1))) {
                         rej = true;
                         k = 0;
                         kp++;
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
                     } else {
                         const float ratio = me / ps->rho0;
                         const bool conv = fabsf(ratio) < ps->eta;
-                        const bool unverified = l.warm && !rej && k == 0;
+                        const bool unverified = warm && !rej && k == 0;
                         const bool done = (conv && k + 1 >= ps->min_it && !unverified) || (k + 1 >= ps->max_it);
                         if (done) {
                             act = ACT_FINAL;
@@ -343,7 +344,7 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
                                 st->iterations = kp + 1;
                                 st->converged = conv ? 1 : 0;
                                 st->max_err_bits = ld_volatile(me_s + kp);
-                                st->warm_used = (l.warm && !rej) ? 1 : 0;
+                                st->warm_used = (warm && !rej) ? 1 : 0;
                                 st->last_k = k;
                             }
                         } else {

@@ -232,7 +232,11 @@ void BatchEngine::build()
     int cap0 = 16;
     for (const Scene& s : sc_) cap0 = std::max(cap0, initial_neighbor_capacity(s.prm));
     built_ = true;
-    if (features_on()) ensure_warm_buffers();
+    auto_on_.assign(sc_.size(), 0);
+    auto_any_ = false;
+    warm_scene_.alloc(sc_.size());
+    upload_auto();
+    if (history_on()) ensure_warm_buffers();
     ensure_neighbors(cap0);
     upload_colliders();
     build_items();
@@ -345,7 +349,7 @@ StepBuffers BatchEngine::buffers(int c)
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
     b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p + sc_.size();
-    b.hist = features_on() ? phist_[c].p : nullptr;
+    b.hist = history_on() ? phist_[c].p : nullptr;
     b.gradrho = features_on() ? gradrho_.p : nullptr;
     return b;
 }
@@ -369,8 +373,8 @@ int BatchEngine::enqueue_step(int c, int grid)
     g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
     g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
     const bool feats = features_on();
-    g.hist_in = feats ? phist_[c].p : nullptr;
-    g.hist_out = feats ? phist_[1 - c].p : nullptr;
+    g.hist_in = history_on() ? phist_[c].p : nullptr;
+    g.hist_out = history_on() ? phist_[1 - c].p : nullptr;
     g.status = status_.p + S;
     launches += launch_grid_order(g, stream_);
     launches += launch_batch_neighbors(a, pos_[1 - c].p, cell_start_.p, nbr_.p, nbr_count_.p, stream_);
@@ -389,10 +393,12 @@ int BatchEngine::enqueue_step(int c, int grid)
             w.mstride = mstride_;
             launches += launch_batch_pci_predict0(a, b, stream_);
             launches += launch_batch_density_first(a, b, w, stream_);
-            if (warm_ == LSP_WARM_MLP) {
-                // The network's guess on the tensor cores, one block per item.
+            if (guess_on()) {
+                // The network's guess on the tensor cores, one block per item (in
+                // LSP_WARM_AUTO only for the scenes switched on).
                 launch_batch_warm_guess_tc(mlp_.umma(), dparams_.p, items_.p, items_count_, b, feat_.p,
-                                           status_.p + S, stream_);
+                                           warm_ == LSP_WARM_AUTO ? warm_scene_.p : nullptr, status_.p + S,
+                                           stream_);
                 launches++;
             }
         }
@@ -402,7 +408,8 @@ int BatchEngine::enqueue_step(int c, int grid)
         l.maxerr = maxerr_.p;
         l.mstride = mstride_;
         l.first_done = feats ? 1 : 0;
-        l.warm = warm_ == LSP_WARM_MLP ? 1 : 0;
+        l.warm = guess_on() ? 1 : 0;
+        l.warm_scene = warm_ == LSP_WARM_AUTO ? warm_scene_.p : nullptr;
         if (!launch_batch_pci_loop(a, b, l, grid, stream_))
             throw Error(LSP_ERR_CUDA, "the cooperative launch of the batch's PCISPH loop was refused");
         launches++;
@@ -490,7 +497,7 @@ void BatchEngine::finish_step(lsp_step_stats* stats)
             local.converged = st.converged;
             local.max_density_error_ratio = (double)me / (double)sc_[s].prm.rest_density;
             local.warm_start_used = st.warm_used;
-            local.warm_start_tried = warm_ == LSP_WARM_MLP ? 1 : 0;
+            local.warm_start_tried = (warm_ == LSP_WARM_MLP || (warm_ == LSP_WARM_AUTO && auto_on_[s])) ? 1 : 0;
             sc_[s].last_k = st.last_k;
             if (sc_[s].prm.strict_convergence && !st.converged) not_converged = true;
         } else {
@@ -500,6 +507,24 @@ void BatchEngine::finish_step(lsp_step_stats* stats)
         local.escaped = (int32_t)st.escaped;
         if (stats) stats[s] = local;
         errors |= st.error_flags;
+    }
+    if (warm_ == LSP_WARM_AUTO && pcisph_) {
+        // A zero-start scene that needed more iterations than its switch point, or missed
+        // eta, uses the guess from the next step on (the single-scene rule, per scene). The
+        // first switch adds the feature pass to the step, so its graph is captured again.
+        bool changed = false;
+        for (int s = 0; s < S; s++) {
+            const int thr = warm_auto_switch(sc_[s].prm);
+            if (!auto_on_[s] && ((int)hstatus_[s].iterations > thr || !hstatus_[s].converged)) {
+                auto_on_[s] = 1;
+                changed = true;
+            }
+        }
+        if (changed) {
+            if (!auto_any_) drop_graphs();
+            auto_any_ = true;
+            upload_auto();
+        }
     }
     if (errors & kErrTimeout) throw Error(LSP_ERR_TIMEOUT, "a grid barrier of the batch's PCISPH loop gave up");
     if (errors & kErrNeighborOverflow) throw Error(LSP_ERR_CAPACITY, "neighbour list overflow persisted after resizing");
@@ -792,20 +817,31 @@ void BatchEngine::ensure_warm_buffers()
 
 void BatchEngine::set_warm_start(int mode)
 {
-    if (mode != LSP_WARM_ZERO && mode != LSP_WARM_MLP)
-        throw Error(LSP_ERR_INVALID, "a batch's warm start is LSP_WARM_ZERO or LSP_WARM_MLP");
-    if (mode == LSP_WARM_MLP && !sc_.empty() && !pcisph_)
+    if (mode != LSP_WARM_ZERO && mode != LSP_WARM_MLP && mode != LSP_WARM_AUTO) throw Error(LSP_ERR_INVALID, "unknown warm_start");
+    if (mode != LSP_WARM_ZERO && !sc_.empty() && !pcisph_)
         throw Error(LSP_ERR_INVALID, "the learned warm start needs PCISPH scenes");
     warm_ = mode;
+    std::fill(auto_on_.begin(), auto_on_.end(), 0);
+    auto_any_ = false;
+    if (built_) upload_auto();
     drop_graphs();
-    if (features_on()) ensure_warm_buffers();
+    if (history_on()) ensure_warm_buffers();
+}
+
+void BatchEngine::upload_auto()
+{
+    if (auto_on_.empty()) return;
+    activate();
+    CK(cudaMemcpyAsync(warm_scene_.p, auto_on_.data(), auto_on_.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       stream_));
+    CK(cudaStreamSynchronize(stream_));
 }
 
 void BatchEngine::mlp_record(bool on)
 {
     record_ = on;
     drop_graphs();
-    if (features_on()) ensure_warm_buffers();
+    if (history_on()) ensure_warm_buffers();
 }
 
 void BatchEngine::mlp_reset(uint64_t seed)

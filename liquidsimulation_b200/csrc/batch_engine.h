@@ -92,7 +92,13 @@ private:
     BatchArgs args();
     void stage(size_t floats);
     void check_scene(int scene) const;
-    bool features_on() const { return pcisph_ && (record_ || warm_ == LSP_WARM_MLP); }
+    // The guess runs for every scene (LSP_WARM_MLP) or for the scenes LSP_WARM_AUTO has
+    // switched on; features are computed whenever some scene uses the guess or recording is
+    // on, and the pressure history is kept from the start in LSP_WARM_AUTO.
+    bool guess_on() const { return pcisph_ && (warm_ == LSP_WARM_MLP || (warm_ == LSP_WARM_AUTO && auto_any_)); }
+    bool features_on() const { return pcisph_ && (record_ || guess_on()); }
+    bool history_on() const { return pcisph_ && (record_ || warm_ != LSP_WARM_ZERO); }
+    void upload_auto();
     void ensure_warm_buffers();
 
     int dev_ = 0;
@@ -133,6 +139,9 @@ private:
 
     int warm_ = LSP_WARM_ZERO;
     bool record_ = false, features_valid_ = false;
+    std::vector<int32_t> auto_on_;    // LSP_WARM_AUTO: scenes whose guess is switched on
+    bool auto_any_ = false;
+    DevArray<int32_t> warm_scene_;    // device copy of auto_on_
     DevArray<float4> phist_[2];   // pressure history (p_{n-1}, p_{n-2}, p_{n-3})
     DevArray<float> feat_, gradrho_, tgt_;
     MlpModel mlp_;

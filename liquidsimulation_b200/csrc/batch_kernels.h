@@ -74,6 +74,7 @@ struct BatchLoopArgs {
     int mstride;
     int first_done;
     int warm;
+    const int32_t* warm_scene;   // per-scene use of the guess (LSP_WARM_AUTO); null: every scene
 };
 // Blocks of a.threads threads that can be co-resident (0: no cooperative launch).
 int batch_loop_max_blocks(int threads, int scenes);

@@ -684,6 +684,11 @@ int initial_neighbor_capacity(const lsp_params& p)
 // regrowth frees and reallocates the whole list and redoes the step, and a large
 // cudaFree / cudaMalloc pair has been measured to take anywhere from 15 to 600 ms, so few
 // large steps beat many small ones.
+int warm_auto_switch(const lsp_params& p)
+{
+    return p.warm_auto_iterations > 0 ? p.warm_auto_iterations : std::max(12, p.pci_max_iterations / 2);
+}
+
 int grown_neighbor_capacity(int needed, int current)
 {
     const int64_t c = std::max<int64_t>((int64_t)needed + needed / 2 + 8, 2 * (int64_t)current);
@@ -769,7 +774,7 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
     // LSP_WARM_AUTO: a zero-start step that needed more iterations than the switch point, or
     // missed eta, turns the learned guess on from the next step.
     if (prm_.warm_start == LSP_WARM_AUTO && !auto_on_ && prm_.solver == LSP_SOLVER_PCISPH &&
-        (local.iterations > (prm_.warm_auto_iterations > 0 ? prm_.warm_auto_iterations : 12) || !local.converged))
+        (local.iterations > warm_auto_switch(prm_) || !local.converged))
         auto_on_ = true;
     if (hstatus_->escaped && domain_from_particles_) grid_valid_ = false;
     if (hstatus_->error_flags & kErrTimeout)

@@ -40,6 +40,8 @@ DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt);
 int initial_neighbor_capacity(const lsp_params& p);
 // Neighbour-list capacity after an overflow of `needed` entries with `current` allocated.
 int grown_neighbor_capacity(int needed, int current);
+// LSP_WARM_AUTO switch point: warm_auto_iterations, or max(12, pci_max_iterations / 2) for 0.
+int warm_auto_switch(const lsp_params& p);
 
 class Engine {
 public:

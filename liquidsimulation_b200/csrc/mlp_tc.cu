@@ -295,11 +295,13 @@ __global__ void __launch_bounds__(kTcRows) k_warm_guess_tc(const MlpUmma* __rest
 __global__ void __launch_bounds__(kTcRows) kb_warm_guess_tc(const MlpUmma* __restrict__ wg,
                                                            const DevParams* __restrict__ sp,
                                                            const BatchItem* __restrict__ items, StepBuffers b,
-                                                           const float* __restrict__ feat, DevStatus* st)
+                                                           const float* __restrict__ feat,
+                                                           const int32_t* __restrict__ warm_scene, DevStatus* st)
 {
     __shared__ TcShared sh;
-    tc_begin(sh, wg);
     const BatchItem it = items[blockIdx.x];
+    if (warm_scene && !warm_scene[it.scene]) return;   // block-uniform: one scene per item
+    tc_begin(sh, wg);
     const DevParams& P = sp[it.scene];
     const float p_scale = P.delta * 0.01f * P.rho0;
     uint32_t parity = 0;
@@ -346,10 +348,11 @@ void launch_warm_guess_tc(const MlpUmma* w, const DevParams& P, const StepBuffer
 }
 
 void launch_batch_warm_guess_tc(const MlpUmma* w, const DevParams* sp, const BatchItem* items, int items_count,
-                                const StepBuffers& b, const float* feat, DevStatus* st, cudaStream_t s)
+                                const StepBuffers& b, const float* feat, const int32_t* warm_scene, DevStatus* st,
+                                cudaStream_t s)
 {
     if (items_count <= 0) return;
-    kb_warm_guess_tc<<<items_count, kTcRows, kTcSmemPad, s>>>(w, sp, items, b, feat, st);
+    kb_warm_guess_tc<<<items_count, kTcRows, kTcSmemPad, s>>>(w, sp, items, b, feat, warm_scene, st);
 }
 
 }  // namespace lsp

@@ -52,7 +52,10 @@ void launch_mlp_forward_tc(const MlpUmma* w, const float* feat, float* out, int 
 void launch_warm_guess_tc(const MlpUmma* w, const DevParams& P, const StepBuffers& b, const float* feat,
                           cudaStream_t s);
 struct BatchItem;
+// warm_scene (may be null: every scene): items of scenes with a zero flag keep the plain
+// first correction.
 void launch_batch_warm_guess_tc(const MlpUmma* w, const DevParams* sp, const BatchItem* items, int items_count,
-                                const StepBuffers& b, const float* feat, DevStatus* st, cudaStream_t s);
+                                const StepBuffers& b, const float* feat, const int32_t* warm_scene, DevStatus* st,
+                                cudaStream_t s);
 
 }  // namespace lsp

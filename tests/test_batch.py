@@ -298,3 +298,32 @@ def test_batch_records_and_trains():
     st = batch.update(dt)
     assert all(s.converged for s in st)
     batch.close()
+
+
+def test_batch_auto_warm_start_switches_per_scene():
+    """LSP_WARM_AUTO in a batch: each scene switches to the learned guess after its own slow
+    step (scene 0 at a low switch point, the others never) and matches a single-scene solver
+    in LSP_WARM_AUTO with the same switch point, bit for bit, including which steps tried the
+    guess."""
+    scs = small_batch(seed=15, count=4)
+    w = _trained_weights(scs[0])
+    for k, sc in enumerate(scs):
+        sc.params.warm_auto_iterations = 2 if k == 0 else 1000
+    batch = batch_from_scenes(scs)
+    batch.mlp_set_weights(w)
+    batch.set_warm_start(abi.LSP_WARM_AUTO)
+    singles = [from_scene(sc) for sc in scs]
+    for s in singles:
+        s.mlp_set_weights(w)
+        s.set_params(warm_start=abi.LSP_WARM_AUTO)
+    dt = scs[0].dt
+    for step in range(4):
+        sb = batch.update(dt)
+        for k, s in enumerate(singles):
+            ss = s.update(dt)
+            assert (sb[k].iterations, sb[k].warm_start_used, sb[k].warm_start_tried, sb[k].converged) == \
+                   (ss.iterations, ss.warm_start_used, ss.warm_start_tried, ss.converged), (step, k)
+            compare_scene(batch, k, s, grid=False, nbrs=(step == 3), tag=f"auto step {step}")
+        assert sb[0].warm_start_tried == (1 if step > 0 else 0)
+        assert all(sb[k].warm_start_tried == 0 for k in range(1, len(scs)) if sb[k].converged)
+    close_all(batch, singles)
