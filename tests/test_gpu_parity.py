@@ -275,3 +275,27 @@ def test_errors_are_reported():
         s.update(0.001)
     assert e.value.code == abi.LSP_ERR_DEVICE_STATUS
     s.close()
+
+
+@pytest.mark.parametrize("loop_mode", [abi.LSP_LOOP_PERSISTENT, abi.LSP_LOOP_HOST])
+def test_coincident_particles(oracle_mod, loop_mode):
+    """Particles added twice at exactly the same position (and some offset along one axis
+    only): their pressure-force direction is 0/0, so the reference's NaN reset zeroes the
+    whole pressure force of those particles (PCISPHSolver.cpp:129-150), and coordinates that
+    differ in one axis give exact zero components elsewhere. Every field must still match
+    the oracle bit for bit."""
+    import dataclasses
+    sc = scenes.dam_break_pcisph(seed=9, counts=(10, 14, 10), s=0.02)
+    sc.params.loop_mode = loop_mode
+    rng = np.random.default_rng(9)
+    pick = rng.choice(sc.n, 40, replace=False)
+    twins = sc.positions[pick].copy()
+    shifted = sc.positions[pick[:10]].copy()
+    shifted[:, 1] += np.float32(0.001)
+    pos = np.concatenate([sc.positions, twins, shifted]).astype(np.float32)
+    sc = dataclasses.replace(sc, positions=pos, velocities=np.zeros_like(pos))
+    gpu, orc = run_pair(oracle_mod, sc, steps=3)
+    pf = gpu.read(abi.FIELD_PRED_PRESSURE_FORCE).reshape(-1, 3)
+    assert np.all(pf[pick] == 0) and np.all(pf[sc.n - 50:sc.n - 10] == 0)
+    gpu.close()
+    orc.close()
