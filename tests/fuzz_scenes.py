@@ -41,4 +41,11 @@ def random_scene(seed):
             cols.append(scenes.Collider("sphere", c, float(rng.uniform(0.03, 0.1)), False))
     domain = ((0.0, 0.0, 0.0), (1.0, 1.0, 1.0)) if rng.integers(2) else None
     dt = float(rng.choice([0.0005, 0.001, 0.002]))
+    # Drawn last so the draws above stay those of earlier versions of this generator. Some
+    # PCISPH scenes repeat a few particles at exactly the same position (0/0 pressure-force
+    # directions, reset by the reference's NaN test); SPH has no such reset, so it gets none.
+    if pci and rng.integers(4) == 0:
+        dup = rng.choice(pos.shape[0], max(1, pos.shape[0] // 50), replace=False)
+        pos = np.concatenate([pos, pos[dup]]).astype(np.float32)
+        vel = np.concatenate([vel, vel[dup]]).astype(np.float32)
     return scenes.Scene(f"fuzz_{seed}", params, pos, vel, cols, dt, 3, domain=domain, spacing=s), pci
