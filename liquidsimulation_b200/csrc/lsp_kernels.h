@@ -120,6 +120,9 @@ void launch_scatter_state(const float* x, const float* v, const float* half, con
                           float4* hvel, float4* oldv, int64_t n, cudaStream_t s);
 // dst[slot_of_id[id]] = (in[3 id], in[3 id + 1], in[3 id + 2], 0) for caller-order rows.
 void launch_scatter_vec(const float* in, const int32_t* slot_of_id, float4* dst, int64_t n, cudaStream_t s);
+
+// SM count of the current device (cached per device).
+int device_sm_count();
 // Writes caller-order x, v, v_half, v_half_old, first from device slots.
 void launch_gather_state(const float4* pos, const float4* vel, const float4* hvel, const float4* oldv,
                          const int32_t* slot_of_id, float* x, float* v, float* half, float* old, int32_t* first,

@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(kThreads) k_pci_density(DevParams P, StepBuffe
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t bm = 0;
-        for (int w = 0; w < kThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) bm = max(bm, __float_as_uint(wmax[w]));
         if (bm) atomicMax(&b.status->max_err_bits, bm);
     }
 }
@@ -58,19 +58,19 @@ __global__ void __launch_bounds__(kThreads) k_pci_force(DevParams P, StepBuffers
     pci_force_one(P, b, SDW, TH, i, b.ppos);
 }
 
-static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 void launch_pci_predict(const DevParams& P, const StepBuffers& b, int iteration, cudaStream_t s)
 {
-    if (P.n) k_pci_predict<<<blocks_for(P.n), kThreads, 0, s>>>(P, b, iteration);
+    if (P.n) k_pci_predict<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b, iteration);
 }
 void launch_pci_density(const DevParams& P, const StepBuffers& b, int iteration, cudaStream_t s)
 {
-    if (P.n) k_pci_density<<<blocks_for(P.n), kThreads, 0, s>>>(P, b, iteration);
+    if (P.n) k_pci_density<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b, iteration);
 }
 void launch_pci_force(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
-    if (P.n) k_pci_force<<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+    if (P.n) k_pci_force<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
 }
 
 // ------------------------------------------------------------------ learned warm start
@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, Ste
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t bm = 0;
-        for (int k = 0; k < kThreads / 32; k++) bm = max(bm, __float_as_uint(wmax[k]));
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) bm = max(bm, __float_as_uint(wmax[k]));
         if (bm) {
             atomicMax(w.maxerr0, bm);
             atomicMax(&b.status->max_err_bits, bm);
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(kThreads) k_pci_density_first(DevParams P, Ste
 
 void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const WarmArgs& w, cudaStream_t s)
 {
-    if (P.n) k_pci_density_first<<<(unsigned)((P.n + kThreads - 1) / kThreads), kThreads, 0, s>>>(P, b, w);
+    if (P.n) k_pci_density_first<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b, w);
 }
 
 // ------------------------------------------------------------------ persistent loop
@@ -142,13 +142,13 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     __syncthreads();
     float4* pp[2] = {b.ppos, ppos_alt};
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    // The particles of a pass: full rounds of one contiguous 1024-particle chunk per block,
+    // The particles of a pass: full rounds of one contiguous blockDim.x chunk per block,
     // then the partial last round split evenly over all blocks (in whole warps), so that no
     // SM runs a whole extra round while the others wait at the next grid barrier. Every pass
     // maps particles to threads the same way (the bounds are recomputed per pass so that
     // they hold no registers across the loop).
     auto for_particles = [&](auto&& f) {
-        const int per_round = (int)gridDim.x * kLoopThreads;
+        const int per_round = (int)(gridDim.x * blockDim.x);
         const int full_end = (P.n / per_round) * per_round;
         const int chunk = ((P.n - full_end + (int)gridDim.x - 1) / (int)gridDim.x + 31) & ~31;
         const int j = full_end + (int)blockIdx.x * chunk + (int)threadIdx.x;
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
         __syncthreads();
         if (threadIdx.x == 0) {
             uint32_t bm = 0;
-            for (int w = 0; w < kLoopThreads / 32; w++) bm = max(bm, __float_as_uint(wmax[w]));
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) bm = max(bm, __float_as_uint(wmax[w]));
             if (bm) atomicMax(&maxerr[slot], bm);
         }
         __syncthreads();
@@ -225,11 +225,22 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     }
 }
 
-// Per device: blocks of k_pci_loop per SM (0: no cooperative launch) and SM count.
+// Per device and block size (1024 / 512 / 256 / 128 threads): resident blocks of k_pci_loop
+// per SM (0: no cooperative launch).
 constexpr int kMaxDevices = 64;
-static int g_loop_blocks_per_sm[kMaxDevices];
-static int g_sm_count[kMaxDevices];
+constexpr int kLoopShapes = 4;
+static int g_loop_blocks_per_sm[kMaxDevices][kLoopShapes];
 static bool g_loop_ready[kMaxDevices];
+
+// Block size of the loop for n particles: the largest of 1024, 512, 256 and 128 that still
+// gives every SM a block (one 1024-thread block per SM is fastest at 1M particles; a
+// 12,000-particle scene in blocks of 1024 would run on 12 SMs).
+static int loop_shape(int64_t n, int sms)
+{
+    int k = 0;
+    while (k + 1 < kLoopShapes && (n + (kLoopThreads >> k) - 1) / (kLoopThreads >> k) < sms) k++;
+    return k;
+}
 
 bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt, void* sync, uint32_t* maxerr,
                      int first_done, int warm, cudaStream_t s, int* grid_used)
@@ -241,22 +252,26 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     if (!g_loop_ready[dev]) {
         int coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        cudaDeviceGetAttribute(&g_sm_count[dev], cudaDevAttrMultiProcessorCount, dev);
-        int per = 0;
-        if (coop && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kLoopThreads, 0) == cudaSuccess)
-            g_loop_blocks_per_sm[dev] = per;
-        else
-            g_loop_blocks_per_sm[dev] = 0;
+        for (int k = 0; k < kLoopShapes; k++) {
+            int per = 0;
+            if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kLoopThreads >> k, 0) !=
+                             cudaSuccess)
+                per = 0;
+            g_loop_blocks_per_sm[dev][k] = per;
+        }
         g_loop_ready[dev] = true;
     }
-    if (g_loop_blocks_per_sm[dev] <= 0) return false;
-    int need = (int)((P.n + kLoopThreads - 1) / kLoopThreads);
-    int grid = std::min(need, g_loop_blocks_per_sm[dev] * g_sm_count[dev]);
+    const int sms = device_sm_count();
+    const int shape = loop_shape(P.n, sms);
+    const int threads = kLoopThreads >> shape;
+    if (g_loop_blocks_per_sm[dev][shape] <= 0) return false;
+    int need = (int)((P.n + threads - 1) / threads);
+    int grid = std::min(need, g_loop_blocks_per_sm[dev][shape] * sms);
     DevParams Pc = P;
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;
     void* args[] = {&Pc, &bc, &ppos_alt, &sy, &maxerr, &first_done, &warm};
-    if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(kLoopThreads), args, 0, s) != cudaSuccess)
+    if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(threads), args, 0, s) != cudaSuccess)
         return false;
     if (grid_used) *grid_used = grid;
     return true;

@@ -62,27 +62,27 @@ __global__ void __launch_bounds__(kThreads) k_integrate_collide(DevParams P, Ste
     integrate_one(P, b, i, add_pforce);
 }
 
-static inline unsigned blocks_for(int64_t n) { return (unsigned)((n + kThreads - 1) / kThreads); }
+static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
-    if (P.n) k_density<<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+    if (P.n) k_density<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
 }
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
     if (!P.n) return;
     if (b.gradrho)
-        k_nonpressure<true><<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+        k_nonpressure<true><<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
     else
-        k_nonpressure<false><<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+        k_nonpressure<false><<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
 }
 void launch_sph_pressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
-    if (P.n) k_sph_pressure<<<blocks_for(P.n), kThreads, 0, s>>>(P, b);
+    if (P.n) k_sph_pressure<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
 }
 void launch_integrate_collide(const DevParams& P, const StepBuffers& b, bool add_pforce, cudaStream_t s)
 {
-    if (P.n) k_integrate_collide<<<blocks_for(P.n), kThreads, 0, s>>>(P, b, add_pforce ? 1 : 0);
+    if (P.n) k_integrate_collide<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b, add_pforce ? 1 : 0);
 }
 
 }  // namespace lsp

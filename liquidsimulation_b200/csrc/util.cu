@@ -217,4 +217,18 @@ void launch_bounds(const float4* pos, int64_t n, int32_t* out, cudaStream_t s)
     if (n) k_bounds<<<148 * 4, kThreads, 0, s>>>(pos, n, out);
 }
 
+int device_sm_count()
+{
+    constexpr int kMaxDevices = 64;
+    static int cached[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
+    if (cached[dev] <= 0) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cached[dev] = sms > 0 ? sms : 148;
+    }
+    return cached[dev];
+}
+
 }  // namespace lsp
