@@ -9,6 +9,8 @@
 #include "lsp_kernels.h"
 #include "particle_ops.cuh"
 
+#include <algorithm>
+
 namespace lsp {
 
 constexpr int kThreads = 256;
@@ -20,9 +22,8 @@ __global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b
     stage_table(W, b.tables, T_W);
     stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    density_one(P, b, W, TH2, i);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x)
+        density_one(P, b, W, TH2, i);
 }
 
 // SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248). The
@@ -35,9 +36,8 @@ __global__ void __launch_bounds__(kThreads) k_nonpressure(DevParams P, StepBuffe
     __shared__ float4 NA[kTableSize], NB[kTableSize];
     stage_nonpressure_slots(NA, NB, b.tables);
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    nonpressure_one<kGrad>(P, b, NA, NB, i);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x)
+        nonpressure_one<kGrad>(P, b, NA, NB, i);
 }
 
 // SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
@@ -64,17 +64,27 @@ __global__ void __launch_bounds__(kThreads) k_integrate_collide(DevParams P, Ste
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// The density and non-pressure passes loop over the particles with a fixed number of blocks
+// per SM, so each block stages its tables once for several particles per thread instead of
+// once per 256 particles (the non-pressure records are 32 KB a block). Measured at 1M
+// particles: 16 blocks per SM for density (4 % faster than one block per 256 particles,
+// 8 per SM was slower), 4 for non-pressure (7 % faster).
+static inline unsigned stride_grid(int64_t n, int per_sm)
+{
+    return std::min<unsigned>(blocks_for(n, kThreads), (unsigned)(per_sm * device_sm_count()));
+}
+
 void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
-    if (P.n) k_density<<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
+    if (P.n) k_density<<<stride_grid(P.n, 16), kThreads, 0, s>>>(P, b);
 }
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
     if (!P.n) return;
     if (b.gradrho)
-        k_nonpressure<true><<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
+        k_nonpressure<true><<<stride_grid(P.n, 4), kThreads, 0, s>>>(P, b);
     else
-        k_nonpressure<false><<<blocks_for(P.n, kThreads), kThreads, 0, s>>>(P, b);
+        k_nonpressure<false><<<stride_grid(P.n, 4), kThreads, 0, s>>>(P, b);
 }
 void launch_sph_pressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
