@@ -125,6 +125,13 @@ typedef struct lsp_solver lsp_solver;
 void lsp_params_default(lsp_params* p);
 const char* lsp_last_error(void);
 int lsp_device_info(int* sm_count, int* cc_major, int* cc_minor);
+/* Check of the bounded wait in the persistent loops' grid barrier (no counterpart in the
+ * reference): on `device` (< 0: current), one barrier round with `blocks` blocks (1..8)
+ * waiting for `parties` arrivals (1..16) and a short spin limit. completed = blocks that
+ * passed; error_flags gets bit 4 (timeout) when a block gave up waiting. With fewer blocks
+ * than parties the round cannot complete: the waits end with the timeout bit instead of a
+ * hang, and the device stays usable. */
+int lsp_barrier_probe(int device, int blocks, int parties, int32_t* completed, uint32_t* error_flags);
 
 /* SPHSolver::SPHSolver / PCISPHSolver::PCISPHSolver (SPHSolver.cpp:9-86). device < 0 = current. */
 int lsp_create(const lsp_params* params, int device, lsp_solver** out);

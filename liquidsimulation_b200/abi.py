@@ -191,6 +191,7 @@ def _declare(lib):
         "lsp_params_default": (None, [POINTER(LspParams)]),
         "lsp_last_error": (c_char_p, []),
         "lsp_device_info": (c_int, [POINTER(c_int), POINTER(c_int), POINTER(c_int)]),
+        "lsp_barrier_probe": (c_int, [c_int, c_int, c_int, POINTER(c_int32), POINTER(c_uint32)]),
         "lsp_create": (c_int, [POINTER(LspParams), c_int, POINTER(c_void_p)]),
         "lsp_destroy": (c_int, [S]),
         "lsp_set_params": (c_int, [S, POINTER(LspParams)]),

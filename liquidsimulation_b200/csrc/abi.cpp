@@ -60,6 +60,28 @@ void lsp_params_default(lsp_params* p)
 
 const char* lsp_last_error(void) { return g_last_error.c_str(); }
 
+int lsp_barrier_probe(int device, int blocks, int parties, int32_t* completed, uint32_t* error_flags)
+{
+    return lsp::guard([&] {
+        if (!completed || !error_flags || blocks < 1 || blocks > 8 || parties < 1 || parties > 16)
+            throw lsp::Error(LSP_ERR_INVALID, "barrier probe: blocks in [1, 8], parties in [1, 16], non-null outputs");
+        int prev = 0;
+        LSP_CK(cudaGetDevice(&prev));
+        if (device >= 0) LSP_CK(cudaSetDevice(device));
+        int done = 0;
+        uint32_t flags = 0;
+        try {
+            lsp::barrier_probe(blocks, parties, &done, &flags);
+        } catch (...) {
+            cudaSetDevice(prev);
+            throw;
+        }
+        LSP_CK(cudaSetDevice(prev));
+        *completed = done;
+        *error_flags = flags;
+    });
+}
+
 int lsp_device_info(int* sm_count, int* cc_major, int* cc_minor)
 {
     return lsp::guard([&] {

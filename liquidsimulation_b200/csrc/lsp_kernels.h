@@ -123,6 +123,9 @@ void launch_scatter_vec(const float* in, const int32_t* slot_of_id, float4* dst,
 
 // SM count of the current device (cached per device).
 int device_sm_count();
+// One bounded grid barrier of `blocks` blocks waiting for `parties` arrivals (test of the
+// loops' timeout path); throws Error on a CUDA failure.
+void barrier_probe(int blocks, int parties, int* completed, uint32_t* error_flags);
 // Writes caller-order x, v, v_half, v_half_old, first from device slots.
 void launch_gather_state(const float4* pos, const float4* vel, const float4* hvel, const float4* oldv,
                          const int32_t* slot_of_id, float* x, float* v, float* half, float* old, int32_t* first,

@@ -10,8 +10,10 @@
 #include "loop_sync.cuh"
 #include "particle_ops.cuh"
 #include "warm_ops.cuh"
+#include "host_util.h"
 
 #include <algorithm>
+#include <string>
 
 namespace lsp {
 
@@ -275,6 +277,48 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
         return false;
     if (grid_used) *grid_used = grid;
     return true;
+}
+
+// ------------------------------------------------------------------ barrier probe
+//
+// One grid barrier with `parties` arrivals per round and a short spin limit, for the test
+// of the bounded wait: with fewer blocks than parties nothing completes the round, the
+// waiting blocks give up, raise kErrTimeout and leave, and the device stays usable.
+__global__ void k_barrier_probe(LoopSync* sy, DevStatus* st, uint32_t parties, unsigned long long limit, int* done)
+{
+    const bool ok = grid_barrier(sy, st, parties, limit);
+    if (threadIdx.x == 0 && ok) atomicAdd(done, 1);
+}
+
+void barrier_probe(int blocks, int parties, int* completed, uint32_t* error_flags)
+{
+    struct Probe {
+        LoopSync sync;
+        DevStatus status;
+        int done;
+    };
+    Probe* d = nullptr;
+    cudaStream_t s = nullptr;
+    cudaError_t e = cudaMalloc((void**)&d, sizeof(Probe));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(Probe), s);
+    if (e == cudaSuccess) {
+        LoopSync* sy = &d->sync;
+        DevStatus* st = &d->status;
+        uint32_t np = (uint32_t)parties;
+        unsigned long long limit = 1ull << 16;
+        int* done = &d->done;
+        void* args[] = {&sy, &st, &np, &limit, &done};
+        e = cudaLaunchCooperativeKernel((const void*)k_barrier_probe, dim3(blocks), dim3(32), args, 0, s);
+    }
+    Probe h{};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, d, sizeof(Probe), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (s) cudaStreamDestroy(s);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) throw Error(LSP_ERR_CUDA, std::string("barrier probe: ") + cudaGetErrorString(e));
+    *completed = h.done;
+    *error_flags = h.status.error_flags;
 }
 
 }  // namespace lsp

@@ -299,3 +299,24 @@ def test_coincident_particles(oracle_mod, loop_mode):
     assert np.all(pf[pick] == 0) and np.all(pf[sc.n - 50:sc.n - 10] == 0)
     gpu.close()
     orc.close()
+
+
+def test_bounded_barrier_gives_up_and_device_stays_usable():
+    """The persistent loops' grid barrier waits with a bounded spin: a round that cannot
+    complete (fewer blocks than parties) ends with the timeout bit instead of a hang, only
+    the block left waiting gives up, and the device keeps working afterwards."""
+    import ctypes
+    lib = abi.load_library()
+    done, flags = ctypes.c_int32(), ctypes.c_uint32()
+    timeout_bit = 4
+    assert lib.lsp_barrier_probe(-1, 4, 4, ctypes.byref(done), ctypes.byref(flags)) == 0
+    assert (done.value, flags.value & timeout_bit) == (4, 0)
+    assert lib.lsp_barrier_probe(-1, 1, 2, ctypes.byref(done), ctypes.byref(flags)) == 0
+    assert (done.value, flags.value & timeout_bit) == (0, timeout_bit)
+    assert lib.lsp_barrier_probe(-1, 3, 2, ctypes.byref(done), ctypes.byref(flags)) == 0
+    assert (done.value, flags.value & timeout_bit) == (2, timeout_bit)
+    assert lib.lsp_barrier_probe(-1, 9, 2, ctypes.byref(done), ctypes.byref(flags)) == abi.LSP_ERR_INVALID
+    sc = scenes.dam_break_pcisph(seed=3, counts=(8, 8, 8), s=0.02)
+    s = from_scene(sc)
+    assert s.update(sc.dt).iterations >= 1
+    s.close()
