@@ -13,6 +13,7 @@
 #include "host_util.h"
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 
 namespace lsp {
@@ -231,8 +232,10 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
 // per SM (0: no cooperative launch).
 constexpr int kMaxDevices = 64;
 constexpr int kLoopShapes = 4;
+// Filled once per device under a lock (solvers on different host threads may launch at once).
 static int g_loop_blocks_per_sm[kMaxDevices][kLoopShapes];
 static bool g_loop_ready[kMaxDevices];
+static std::mutex g_loop_mutex;
 
 // Block size of the loop for n particles: the largest of 1024, 512, 256 and 128 that still
 // gives every SM a block (one 1024-thread block per SM is fastest at 1M particles; a
@@ -251,6 +254,7 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     if (P.n <= 0 || P.max_it <= 0) return false;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+    std::unique_lock<std::mutex> lock(g_loop_mutex);
     if (!g_loop_ready[dev]) {
         int coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
@@ -266,9 +270,11 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     const int sms = device_sm_count();
     const int shape = loop_shape(P.n, sms);
     const int threads = kLoopThreads >> shape;
-    if (g_loop_blocks_per_sm[dev][shape] <= 0) return false;
+    const int per_sm = g_loop_blocks_per_sm[dev][shape];
+    lock.unlock();
+    if (per_sm <= 0) return false;
     int need = (int)((P.n + threads - 1) / threads);
-    int grid = std::min(need, g_loop_blocks_per_sm[dev][shape] * sms);
+    int grid = std::min(need, per_sm * sms);
     DevParams Pc = P;
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;

@@ -5,6 +5,8 @@
 #include "lsp_device.cuh"
 #include "lsp_kernels.h"
 
+#include <atomic>
+
 namespace lsp {
 
 constexpr int kThreads = 256;
@@ -220,15 +222,17 @@ void launch_bounds(const float4* pos, int64_t n, int32_t* out, cudaStream_t s)
 int device_sm_count()
 {
     constexpr int kMaxDevices = 64;
-    static int cached[kMaxDevices];
+    static std::atomic<int> cached[kMaxDevices];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 148;
-    if (cached[dev] <= 0) {
+    int v = cached[dev].load(std::memory_order_relaxed);
+    if (v <= 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cached[dev] = sms > 0 ? sms : 148;
+        v = sms > 0 ? sms : 148;
+        cached[dev].store(v, std::memory_order_relaxed);
     }
-    return cached[dev];
+    return v;
 }
 
 }  // namespace lsp
