@@ -731,11 +731,12 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
         g.hist_in = phist_[cur_].p; g.hist_out = phist_[1 - cur_].p;
         g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
+        // The neighbour build also sums the start-of-step density (k_neighbors_density).
+        g.tables = tables_.p; g.rho = rho_.p; g.pres = pres_.p;
         timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_sort(g, stream_); });
         timed(LSP_PROF_NEIGHBORS, [&] { return launch_neighbors(g, stream_); });
         cur_ = 1 - cur_;
         StepBuffers b = buffers();
-        timed(LSP_PROF_DENSITY, [&] { launch_density(P, b, stream_); return 1; });
         timed(LSP_PROF_NONPRESSURE, [&] { launch_nonpressure(P, b, stream_); return 1; });
         if (prm_.solver == LSP_SOLVER_SPH) {
             timed(LSP_PROF_SPH_PRESSURE, [&] { launch_sph_pressure(P, b, stream_); return 1; });

@@ -188,6 +188,36 @@ __global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const u
     record_neighbor_count(P, c, valid, st);
 }
 
+// The same lists plus the start-of-step density and pressure of density_one
+// (SPHSolver::calcParticleDensityPressure, SPHSolver.cpp:442-463), summed while the list is
+// built: the pass over the stored list and its position gathers disappear. (A list that
+// overflows its capacity raises the overflow flag and the step is redone, so the sum over
+// every accepted pair never differs from the stored list's.)
+__global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
+                                    const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
+                                    int32_t* __restrict__ count, DevStatus* st, const float* __restrict__ tables,
+                                    float* __restrict__ rho, float* __restrict__ pres)
+{
+    __shared__ float W[kTableSize], TH2[kTableSize + 1];
+    stage_table(W, tables, T_W);
+    stage_table(TH2, tables, T_THRESH2);
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < P.n;
+    int c = 0;
+    if (valid) {
+        float sum;
+        c = neighbors_one<true>(P, pos, cell_start, nbr, i, W, TH2, &sum);
+        count[i] = min(c, P.nbr_cap);
+        const float r = P.mass * sum;
+        float pr = P.stiffness * (r - P.rho0);
+        if (pr < 0.f) pr *= P.neg;
+        rho[i] = r;
+        pres[i] = pr;
+    }
+    record_neighbor_count(P, c, valid, st);
+}
+
 // ------------------------------------------------------------------ launchers
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -229,7 +259,11 @@ int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;
     if (a.P.n <= 0) return 0;
-    k_neighbors<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
+    if (a.rho)
+        k_neighbors_density<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
+                                                               a.status, a.tables, a.rho, a.pres);
+    else
+        k_neighbors<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
     return 1;
 }
 

@@ -31,6 +31,11 @@ struct GridBuildArgs {
     int32_t* nbr;
     int32_t* nbr_count;
     DevStatus* status;
+    // Optional: the start-of-step density computed in the neighbour build (rho, p written,
+    // tables = the kernel table block); null rho = lists only.
+    const float* tables;
+    float* rho;
+    float* pres;
 };
 
 struct MlpPacked;
@@ -77,7 +82,6 @@ int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
 int launch_grid_order(const GridBuildArgs& a, cudaStream_t s);
 int launch_neighbors(const GridBuildArgs& a, cudaStream_t s);
 
-void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // With b.gradrho set, also stores |grad rho| (a warm-start feature).
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 void launch_sph_pressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);

@@ -58,11 +58,16 @@ __device__ __forceinline__ uint32_t cell_key(const DevParams& P, const float4& p
 // including i, in the reference's order (SPHSpatialGrid::findNeighborParticles,
 // SPHSpatialGrid.cpp:39-76): cell ranges from (x -+ h) / h per axis, x then y rows,
 // each row a contiguous z-run of the sorted array. Stores at most nbr_cap entries and
-// returns the true count.
+// returns the true count. With kDensity it also sums W over the accepted pairs in list
+// order from their squared distances, the sum density_one forms over the stored list
+// (|x_i - x_j|^2 equals |x_j - x_i|^2 bit for bit; W and TH2 as in density_one).
+template <bool kDensity = false>
 __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* __restrict__ pos,
                                              const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
-                                             int i)
+                                             int i, const float* W = nullptr, const float* TH2 = nullptr,
+                                             float* wsum = nullptr)
 {
+    float sum = 0.f;
     const float4 pi = pos[i];
     const V3 xi = v3(pi);
     const float h = P.h;
@@ -91,7 +96,9 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
                 int32_t q = (int32_t)beg;
                 for (const float4* pq = pos + beg; pq < pe; pq++, q++) {
                     const V3 dq = xi - v3(*pq);
-                    if (sqmag(dq) <= P.h2) {
+                    const float s = sqmag(dq);
+                    if (s <= P.h2) {
+                        if (kDensity) sum += lookup_sq(W, TH2, s, P);
                         if (c < cap) {
                             *out = q;
                             out += stride;
@@ -102,6 +109,7 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
             }
         }
     }
+    if (kDensity) *wsum = sum;
     return c;
 }
 

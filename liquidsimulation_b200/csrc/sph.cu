@@ -1,10 +1,10 @@
-// SPH passes over the start-of-step neighbour lists: density/pressure, non-pressure
-// forces (gravity, surface tension, viscosity), the SPH pressure force, and the fused
-// leapfrog integration + collision pass.
+// SPH passes over the start-of-step neighbour lists: non-pressure forces (gravity,
+// surface tension, viscosity), the SPH pressure force, and the fused leapfrog integration +
+// collision pass (the density and pressure are summed in the neighbour build, grid.cu).
 //
 // Thread per particle; each thread walks its own neighbour list in the reference's
 // order, so its sums round exactly as the reference CPU solver's do. The lookup tables
-// the pass needs are staged in shared memory (4 KB each) once per block.
+// the pass needs are staged in shared memory once per block.
 #include "lsp_device.cuh"
 #include "lsp_kernels.h"
 #include "particle_ops.cuh"
@@ -14,17 +14,6 @@
 namespace lsp {
 
 constexpr int kThreads = 256;
-
-// SPHSolver::calcParticleDensityPressure, CPU branch (SPHSolver.cpp:442-463).
-__global__ void __launch_bounds__(kThreads) k_density(DevParams P, StepBuffers b)
-{
-    __shared__ float W[kTableSize], TH2[kTableSize + 1];
-    stage_table(W, b.tables, T_W);
-    stage_table(TH2, b.tables, T_THRESH2);
-    __syncthreads();
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n; i += gridDim.x * blockDim.x)
-        density_one(P, b, W, TH2, i);
-}
 
 // SPHSolver::accumulateNonPressureForces, CPU branch (SPHSolver.cpp:201-248). The
 // reference walks the list up to three times (normal, colour Laplacian when the normal
@@ -64,20 +53,14 @@ __global__ void __launch_bounds__(kThreads) k_integrate_collide(DevParams P, Ste
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
-// The density and non-pressure passes loop over the particles with a fixed number of blocks
-// per SM, so each block stages its tables once for several particles per thread instead of
-// once per 256 particles (the non-pressure records are 32 KB a block). Measured at 1M
-// particles: 16 blocks per SM for density (4 % faster than one block per 256 particles,
-// 8 per SM was slower), 4 for non-pressure (7 % faster).
+// The non-pressure pass loops over the particles with four blocks per SM, so each block
+// stages its tables (32 KB of slot records) once for several particles per thread instead
+// of once per 256 particles: 7 % faster at 1M particles.
 static inline unsigned stride_grid(int64_t n, int per_sm)
 {
     return std::min<unsigned>(blocks_for(n, kThreads), (unsigned)(per_sm * device_sm_count()));
 }
 
-void launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s)
-{
-    if (P.n) k_density<<<stride_grid(P.n, 16), kThreads, 0, s>>>(P, b);
-}
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s)
 {
     if (!P.n) return;
