@@ -67,27 +67,13 @@ __global__ void __launch_bounds__(T) kb_keys(BatchArgs a, const float4* __restri
     record_key_flags(valid, escaped, bad, a.st + it.scene);
 }
 
+// The lists plus the start-of-step density and pressure (k_neighbors_density in grid.cu),
+// per item with the item's scene constants and tables.
 template <int T>
-__global__ void __launch_bounds__(T) kb_neighbors(BatchArgs a, const float4* __restrict__ pos,
-                                                  const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
-                                                  int32_t* __restrict__ count)
-{
-    __shared__ DevParams P;
-    const BatchItem it = a.items[blockIdx.x];
-    stage_params(&P, a.sp, it.scene);
-    __syncthreads();
-    const int i = it.begin + (int)threadIdx.x;
-    const bool valid = i < it.end;
-    int c = 0;
-    if (valid) {
-        c = neighbors_one(P, pos, cell_start, nbr, i);
-        count[i] = min(c, P.nbr_cap);
-    }
-    record_neighbor_count(P, c, valid, a.st + it.scene);
-}
-
-template <int T>
-__global__ void __launch_bounds__(T) kb_density(BatchArgs a, StepBuffers b)
+__global__ void __launch_bounds__(T) kb_neighbors_density(BatchArgs a, const float4* __restrict__ pos,
+                                                          const uint32_t* __restrict__ cell_start,
+                                                          int32_t* __restrict__ nbr, int32_t* __restrict__ count,
+                                                          float* __restrict__ rho, float* __restrict__ pres)
 {
     __shared__ DevParams P;
     __shared__ float W[kTableSize], TH2[kTableSize + 1];
@@ -98,8 +84,19 @@ __global__ void __launch_bounds__(T) kb_density(BatchArgs a, StepBuffers b)
     stage_table(TH2, tb, T_THRESH2);
     __syncthreads();
     const int i = it.begin + (int)threadIdx.x;
-    if (i >= it.end) return;
-    density_one(P, b, W, TH2, i);
+    const bool valid = i < it.end;
+    int c = 0;
+    if (valid) {
+        float sum;
+        c = neighbors_one<true>(P, pos, cell_start, nbr, i, W, TH2, &sum);
+        count[i] = min(c, P.nbr_cap);
+        const float r = P.mass * sum;
+        float pr = P.stiffness * (r - P.rho0);
+        if (pr < 0.f) pr *= P.neg;
+        rho[i] = r;
+        pres[i] = pr;
+    }
+    record_neighbor_count(P, c, valid, a.st + it.scene);
 }
 
 template <int T, bool kGrad>
@@ -426,18 +423,12 @@ int launch_batch_keys(const BatchArgs& a, const float4* pos, uint32_t* key, uint
     return 1;
 }
 
-int launch_batch_neighbors(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
-                           int32_t* count, cudaStream_t s)
+int launch_batch_neighbors_density(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
+                                   int32_t* count, float* rho, float* pres, cudaStream_t s)
 {
     if (!a.items_count) return 0;
-    LSP_BATCH_DISPATCH(a.threads, (kb_neighbors<T><<<a.items_count, T, 0, s>>>(a, pos, cell_start, nbr, count)));
-    return 1;
-}
-
-int launch_batch_density(const BatchArgs& a, const StepBuffers& b, cudaStream_t s)
-{
-    if (!a.items_count) return 0;
-    LSP_BATCH_DISPATCH(a.threads, (kb_density<T><<<a.items_count, T, 0, s>>>(a, b)));
+    LSP_BATCH_DISPATCH(a.threads, (kb_neighbors_density<T><<<a.items_count, T, 0, s>>>(a, pos, cell_start, nbr,
+                                                                                      count, rho, pres)));
     return 1;
 }
 

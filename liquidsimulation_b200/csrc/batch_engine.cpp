@@ -377,9 +377,9 @@ int BatchEngine::enqueue_step(int c, int grid)
     g.hist_out = history_on() ? phist_[1 - c].p : nullptr;
     g.status = status_.p + S;
     launches += launch_grid_order(g, stream_);
-    launches += launch_batch_neighbors(a, pos_[1 - c].p, cell_start_.p, nbr_.p, nbr_count_.p, stream_);
     StepBuffers b = buffers(1 - c);
-    launches += launch_batch_density(a, b, stream_);
+    launches += launch_batch_neighbors_density(a, pos_[1 - c].p, cell_start_.p, nbr_.p, nbr_count_.p, rho_.p,
+                                               pres_.p, stream_);
     launches += launch_batch_nonpressure(a, b, stream_);
     if (pcisph_) {
         CK(cudaMemsetAsync(loop_sync_.p, 0, 4 * sizeof(uint32_t), stream_));

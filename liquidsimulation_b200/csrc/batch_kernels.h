@@ -44,9 +44,9 @@ bool batch_threads_supported(int threads);
 
 int launch_batch_keys(const BatchArgs& a, const float4* pos, uint32_t* key, uint32_t* slot, uint32_t* hist,
                       cudaStream_t s);
-int launch_batch_neighbors(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
-                           int32_t* count, cudaStream_t s);
-int launch_batch_density(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
+// Lists plus the start-of-step density and pressure (rho, pres), per item.
+int launch_batch_neighbors_density(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
+                                   int32_t* count, float* rho, float* pres, cudaStream_t s);
 int launch_batch_nonpressure(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
 int launch_batch_sph_pressure(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
 int launch_batch_integrate(const BatchArgs& a, const StepBuffers& b, bool add_pforce, cudaStream_t s);
