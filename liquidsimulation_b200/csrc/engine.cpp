@@ -745,7 +745,9 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
             local.converged = 1;
         } else {
             device_loop = pcisph_loop(P, b, &local);
-            timed(LSP_PROF_INTEGRATE, [&] { launch_integrate_collide(P, b, true, stream_); return 1; });
+            // The persistent loop integrates in its last pass; the per-phase loop does not.
+            if (!device_loop)
+                timed(LSP_PROF_INTEGRATE, [&] { launch_integrate_collide(P, b, true, stream_); return 1; });
         }
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hstatus_, status_.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_));

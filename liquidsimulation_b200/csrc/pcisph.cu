@@ -118,7 +118,8 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 //   predict(0)
 //   for k: | barrier | density(k) + block max |error| -> maxerr[k] | barrier |
 //          decide (all threads read maxerr[k]): done = (converged && k+1 >= min) || k+1 == max
-//          force(k), and when not done predict(k+1) in the same pass
+//          force(k), and when not done predict(k+1) in the same pass, else the
+//          integration and collisions of the step
 //
 // force(k) reads the predicted positions of iteration k while predict(k+1) writes
 // those of k+1, so x* is double-buffered (ppos, ppos_alt by iteration parity). Every
@@ -210,7 +211,12 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
         const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
         for_particles([&](int i) {
             pci_force_one(P, b, SDW, TH, i, pp[k & 1]);
+            // The last pass also integrates and collides the particle (SPHParticle::integrate
+            // after the loop, PCISPHSolver.cpp:166-169): it reads only the particle's own
+            // state and pressure force, which this thread has just written, and no thread of
+            // this pass reads what it writes (the force pass reads predicted positions).
             if (!done) pci_predict_one(P, b, i, k + 1, pp[(k + 1) & 1]);
+            else integrate_one(P, b, i, 1);
         });
         if (done) break;
         if (!grid_barrier(sy, b.status)) return;
