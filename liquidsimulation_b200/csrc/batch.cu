@@ -375,7 +375,10 @@ __global__ void __launch_bounds__(T, 1024 / T) kb_pci_loop(BatchArgs a, StepBuff
                 pci_force_one(P, b, SDW, TH, i, pp(k - 1));
                 pci_predict_one(P, b, i, k, pp(k));
             } else {
+                // The scene's last pass: force, then integration and collisions (own data
+                // only; the scenes never read each other's particles).
                 pci_force_one(P, b, SDW, TH, i, pp(k));
+                integrate_one(P, b, i, 1);
             }
         });
         if (preB[S] == 0) break;

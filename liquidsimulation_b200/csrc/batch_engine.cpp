@@ -412,8 +412,7 @@ int BatchEngine::enqueue_step(int c, int grid)
         l.warm_scene = warm_ == LSP_WARM_AUTO ? warm_scene_.p : nullptr;
         if (!launch_batch_pci_loop(a, b, l, grid, stream_))
             throw Error(LSP_ERR_CUDA, "the cooperative launch of the batch's PCISPH loop was refused");
-        launches++;
-        launches += launch_batch_integrate(a, b, true, stream_);
+        launches++;   // the loop integrates each scene in its last pass
     } else {
         launches += launch_batch_sph_pressure(a, b, stream_);
         launches += launch_batch_integrate(a, b, false, stream_);
