@@ -315,7 +315,7 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 {
     const V3 xi = v3(ppos[i]);
     float sum = 0.f;
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<3>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return ppos[j]; },
                          [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
     float pd = P.mass * sum;
