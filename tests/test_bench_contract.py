@@ -1,0 +1,52 @@
+"""bench.py's output: one JSON line per run with the keys, types and relations the benchmark
+reports, for the reference arm (on the CPU) and for this library's arm (on a B200), on short
+runs."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+COMMON = {"metric": str, "value": float, "unit": str, "n_gpus": int, "steps": int, "warmup": int,
+          "ms_per_step": float, "higher_is_better": bool, "scaling": str, "dtype": str, "data": str,
+          "config": dict}
+
+
+def _line(args, timeout):
+    r = subprocess.run([sys.executable, "bench.py", *args], cwd=ROOT, capture_output=True, text=True,
+                       timeout=timeout)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout[-2000:]
+    d = json.loads(lines[0])
+    for k, t in COMMON.items():
+        assert isinstance(d[k], (int, float) if t is float else t), (k, d.get(k))
+    assert d["value"] > 0 and d["higher_is_better"] is True and "vs_baseline" in d
+    assert d["config"]["workload"].startswith("wave_breaker_991440")
+    return d
+
+
+def test_reference_arm_line():
+    d = _line(["--impl", "reference", "--steps", "1", "--warmup", "1"], 900)
+    assert d["impl"] == "reference"
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
+    assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+@pytest.mark.gpu
+def test_library_arm_line():
+    d = _line(["--steps", "3", "--warmup", "3", "--train-steps", "5", "--long-steps", "0"], 1200)
+    assert d["n_gpus"] == 1 and d["steps"] == 3 and d["warmup"] == 3 and d["dtype"] == "f32"
+    r = d["roofline"]
+    assert r["bound"] in ("hbm", "tensor") and r["unit"] in ("GB/s", "TFLOP/s")
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-3 and r["traffic"] > 0
+    e = d["e2e"]
+    assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    assert d["gpu_launches"] > 0
+    c = d["clocks"]
+    assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(c) and c["samples"] > 0
+    cb = d["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["value"] > 0
