@@ -488,6 +488,13 @@ void Engine::timed(int cls, F&& launch)
         launches_ += launch();
         return;
     }
+    // The event pairs are summed when the profile is read (profile_read / profile), not
+    // after every step, so a profiled step adds only the event records; a long profiled run
+    // folds its backlog in every 1024 launches.
+    if (pending_.size() >= 1024) {
+        CK(cudaStreamSynchronize(stream_));
+        collect_profile();
+    }
     while (evpool_.size() < evnext_ + 2) {
         cudaEvent_t e;
         CK(cudaEventCreate(&e));
@@ -752,7 +759,6 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(hstatus_, status_.p, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream_));
         CK(cudaStreamSynchronize(stream_));
-        if (profile_) collect_profile();
         if ((hstatus_->error_flags & kErrNeighborOverflow) && attempt < 3) {
             cur_ = 1 - cur_;   // the gather left the pre-step state untouched: redo the step
             ensure_neighbors(grown_neighbor_capacity((int)hstatus_->max_neighbors, nbr_cap_));
