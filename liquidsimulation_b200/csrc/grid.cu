@@ -174,23 +174,10 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
     sorted_key[dest] = k;
 }
 
-// Start-of-step neighbour lists (neighbors_one), column-major.
-__global__ void k_neighbors(DevParams P, const float4* __restrict__ pos, const uint32_t* __restrict__ cell_start,
-                            int32_t* __restrict__ nbr, int32_t* __restrict__ count, DevStatus* st)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = i < P.n;
-    int c = 0;
-    if (valid) {
-        c = neighbors_one(P, pos, cell_start, nbr, i);
-        count[i] = min(c, P.nbr_cap);
-    }
-    record_neighbor_count(P, c, valid, st);
-}
-
-// The same lists plus the start-of-step density and pressure of density_one
-// (SPHSolver::calcParticleDensityPressure, SPHSolver.cpp:442-463), summed while the list is
-// built: the pass over the stored list and its position gathers disappear. (A list that
+// Start-of-step neighbour lists (neighbors_one, column-major) plus the start-of-step density
+// and pressure of density_one (SPHSolver::calcParticleDensityPressure,
+// SPHSolver.cpp:442-463), summed while the list is built: a pass over the stored list and
+// its position gathers would cost more. (A list that
 // overflows its capacity raises the overflow flag and the step is redone, so the sum over
 // every accepted pair never differs from the stored list's.)
 __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
@@ -259,11 +246,8 @@ int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;
     if (a.P.n <= 0) return 0;
-    if (a.rho)
-        k_neighbors_density<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
-                                                               a.status, a.tables, a.rho, a.pres);
-    else
-        k_neighbors<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count, a.status);
+    k_neighbors_density<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
+                                                           a.status, a.tables, a.rho, a.pres);
     return 1;
 }
 

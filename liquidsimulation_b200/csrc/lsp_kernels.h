@@ -31,8 +31,8 @@ struct GridBuildArgs {
     int32_t* nbr;
     int32_t* nbr_count;
     DevStatus* status;
-    // Optional: the start-of-step density computed in the neighbour build (rho, p written,
-    // tables = the kernel table block); null rho = lists only.
+    // The start-of-step density is computed in the neighbour build (rho, p written;
+    // tables = the kernel table block).
     const float* tables;
     float* rho;
     float* pres;
