@@ -18,7 +18,8 @@
 //   k_scatter     particle -> (cell start + slot)
 //   k_rank_gather deterministic rank by caller id inside each cell, then one gather of
 //                 the 64-byte persistent state into the new order
-//   k_neighbors   the start-of-step neighbour lists, column-major, reference order
+//   k_neighbors_density  the start-of-step neighbour lists, column-major, reference
+//                 order, with the density and pressure summed over the accepted pairs
 #include "lsp_kernels.h"
 #include "particle_ops.cuh"
 
