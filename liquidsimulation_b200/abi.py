@@ -276,7 +276,7 @@ def _declare(lib):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    # Optional entry points (declared when present in this build).
+    # Optional entry points (declared when the loaded library exports them).
     for name, (res, args) in EXTRA_SIGNATURES.items():
         fn = getattr(lib, name, None)
         if fn is not None:

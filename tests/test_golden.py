@@ -1,7 +1,7 @@
 """Golden fixtures produced by the reference's own CPU solver (tests/golden/make_golden.py).
 
 The CPU test pins the oracle restatement to them; the GPU test pins the CUDA path
-to them directly, so the GPU box (which has no reference sources) still checks
+to them directly, so a GPU machine without the reference sources still checks
 against the reference's outputs. Tolerance: exact float32 bit equality.
 """
 import json
