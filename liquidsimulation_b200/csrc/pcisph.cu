@@ -144,7 +144,9 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     stage_table(TH, b.tables, T_THRESH);
     stage_table(TH2, b.tables, T_THRESH2);
     __syncthreads();
-    float4* pp[2] = {b.ppos, ppos_alt};
+    // x* of iteration parity 0 / 1. A select, not a two-pointer array: an array indexed by
+    // the iteration lives in local memory, and reading it per particle cost the loop 3.8 %.
+    auto pp = [&](int parity) { return parity ? ppos_alt : b.ppos; };
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     // The particles of a pass: full rounds of one contiguous blockDim.x chunk per block,
     // then the partial last round split evenly over all blocks (in whole warps), so that no
@@ -168,7 +170,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     // density(k) over all particles; the block maximum of |error| goes to maxerr[slot].
     auto density_pass = [&](int k, int slot) {
         float m = 0.f;
-        for_particles([&](int i) { m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp[k & 1])); });
+        for_particles([&](int i) { m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp(k & 1))); });
         uint32_t mb = __float_as_uint(m);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, off));
@@ -185,7 +187,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     int k = 0, kp = 0;
     bool conv = false, rejected = false;
     if (!first_done) {
-        for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp[0]); });
+        for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp(0)); });
         if (!grid_barrier(sy, b.status)) return;
         density_pass(0, 0);
         if (!grid_barrier(sy, b.status)) return;
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
             rejected = true;
             k = 0;
             kp++;
-            for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp[0]); });
+            for_particles([&](int i) { pci_predict_one(P, b, i, 0, pp(0)); });
             if (!grid_barrier(sy, b.status)) return;
             density_pass(0, kp);
             if (!grid_barrier(sy, b.status)) return;
@@ -210,12 +212,12 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
         const bool unverified = warm && !rejected && k == 0;
         const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
         for_particles([&](int i) {
-            pci_force_one(P, b, SDW, TH, i, pp[k & 1]);
+            pci_force_one(P, b, SDW, TH, i, pp(k & 1));
             // The last pass also integrates and collides the particle (SPHParticle::integrate
             // after the loop, PCISPHSolver.cpp:166-169): it reads only the particle's own
             // state and pressure force, which this thread has just written, and no thread of
             // this pass reads what it writes (the force pass reads predicted positions).
-            if (!done) pci_predict_one(P, b, i, k + 1, pp[(k + 1) & 1]);
+            if (!done) pci_predict_one(P, b, i, k + 1, pp((k + 1) & 1));
             else integrate_one(P, b, i, 1);
         });
         if (done) break;
