@@ -223,9 +223,12 @@ int lsp_read_features(lsp_solver* s, float* out, int64_t n);
  * targets float[n], grad float[LSP_MLP_PARAMS], loss float[1], the mean 0.5 r^2), and the
  * per-warp partial sums use a fixed scratch array inside the library (2.7 MiB on each
  * device that loads it, kept until the process exits). n <= 16777216 (LSP_ERR_CAPACITY
- * beyond). Work is queued on the solver's stream; synchronise before reading the outputs.
- * The first call on a device looks up the scratch address and should come before any
- * stream capture. Calls that overlap on the GPU share the scratch and race.
+ * beyond). The buffers must belong to the solver's GPU (or be managed memory).
+ * Work is queued on the solver's stream and is not ordered after work on any other stream:
+ * the inputs must be complete before the call (synchronise the stream that wrote them), and
+ * the outputs may be read only after lsp_synchronize. The scratch address is looked up, and
+ * the module holding it loaded, when the solver is created (lsp_create), so a call itself
+ * allocates nothing. Calls that overlap on the GPU share the scratch and race.
  * No counterpart in the reference. */
 int lsp_mlp_gradient_static(lsp_solver* s, const float* features, const float* targets, int64_t n,
                             float* grad, float* loss);

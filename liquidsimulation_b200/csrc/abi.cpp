@@ -105,7 +105,11 @@ int lsp_create(const lsp_params* params, int device, lsp_solver** out)
         lsp_solver* s = new lsp_solver{nullptr};
         try {
             s->e = new lsp::Engine(*params, device);
+            // The allocation-free gradient's scratch is set up with the solver, so that
+            // lsp_mlp_gradient_static itself never loads a module or looks a symbol up.
+            lsp::scratch_on(s->e->device());
         } catch (...) {
+            delete s->e;
             delete s;
             throw;
         }

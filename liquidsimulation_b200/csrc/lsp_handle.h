@@ -15,6 +15,10 @@ namespace lsp {
 // Sets the message lsp_last_error() returns on this thread.
 void set_last_error(const std::string& message);
 
+// Device address of lsp_mlp_gradient_static's fixed scratch array on `device`, which must be
+// the current device (looked up once per device; mlp_static.cu).
+float* scratch_on(int device);
+
 // Runs an entry point's body: LSP_OK, or the status code of the error it threw with the
 // message kept for lsp_last_error() (host allocation failures map to LSP_ERR_CAPACITY).
 template <typename F>

@@ -35,8 +35,13 @@ constexpr int kMaxDevices = 64;
 // Per-warp partial gradients (kStaticRows x kMlpParams) followed by per-warp losses.
 static __device__ __align__(256) float g_static_grad_scratch[kStaticRows * kMlpParams + kStaticRows];
 
+}  // namespace
+
 // Device address of the scratch array, looked up once per device with that device current:
 // in host code the array's name is only a host-side stand-in, never a device address.
+// lsp_create calls it for the solver's device, so the lookup (and the loading of this
+// file's module with the array, which CUDA's lazy module loading defers to the first use of
+// a symbol) happens when the solver is created, not inside lsp_mlp_gradient_static.
 float* scratch_on(int device)
 {
     static std::mutex mu;
@@ -57,6 +62,8 @@ float* scratch_on(int device)
     return addr[device];
 }
 
+namespace {
+
 // Sums the partial rows in a fixed order: grad[p] = sum_r partial[r][p], loss = sum_r loss[r] / n.
 __global__ void k_static_reduce(const float* __restrict__ scratch, int rows, float inv_n, float* __restrict__ grad,
                                 float* __restrict__ loss)
@@ -74,14 +81,18 @@ __global__ void k_static_reduce(const float* __restrict__ scratch, int rows, flo
     grad[p] = g;
 }
 
-bool on_device(const void* p)
+// Device memory of `device` itself, or managed memory (reachable from every device). Memory
+// of another GPU is refused: the kernels would read it from this device, which faults without
+// peer access and crosses NVLink silently with it.
+bool on_device(const void* p, int device)
 {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type == cudaMemoryTypeManaged) return true;
+    return a.type == cudaMemoryTypeDevice && a.device == device;
 }
 
 }  // namespace
@@ -100,7 +111,8 @@ extern "C" int lsp_mlp_gradient_static(lsp_solver* s, const float* features, con
         lsp::Engine& e = *s->e;
         if (cudaSetDevice(e.device()) != cudaSuccess) throw lsp::Error(LSP_ERR_CUDA, "cudaSetDevice failed");
         for (const void* p : {(const void*)features, (const void*)targets, (const void*)grad, (const void*)loss})
-            if (!lsp::on_device(p)) throw lsp::Error(LSP_ERR_INVALID, "buffers must be device memory");
+            if (!lsp::on_device(p, e.device()))
+                throw lsp::Error(LSP_ERR_INVALID, "buffers must be device memory of the solver's GPU");
         float* scratch = lsp::scratch_on(e.device());
         cudaStream_t st = e.stream();
         // Every partial row and loss slot the reduction reads is written by this launch

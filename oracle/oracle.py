@@ -104,6 +104,7 @@ def _orc_lib():
             "orc_update_box": (c_int, [V, c_int, _fp, _fp]), "orc_update_sphere": (c_int, [V, c_int, _fp, c_float]),
             "orc_count": (c_int64, [V]),
             "orc_step": (c_int, [V, c_float, POINTER(abi.LspStepStats)]),
+            "orc_set_initial_pressure": (c_int, [V, _fp, c_int64]),
             "orc_get": (c_int, [V, c_int, _fp]), "orc_get_f64": (c_int, [V, c_int, POINTER(c_double)]),
             "orc_set_state": (c_int, [V, _fp, _fp, _fp, _fp, _i32p]),
             "orc_mass": (c_float, [V]), "orc_kernel_radius": (c_float, [V]), "orc_delta": (c_float, [V, c_float]),
@@ -258,7 +259,14 @@ class OracleSolver:
     def update_sphere(self, index, center, radius):
         self.L.orc_update_sphere(self.h, index, _f(np.asarray(center, np.float32)), float(radius))
 
-    def step(self, dt):
+    def step(self, dt, initial_pressure=None):
+        """One step. initial_pressure (caller order, float32[n]): the pressure iteration 0
+        takes in place of its own correction, as the device's learned warm start does
+        (checked at iteration 1 and dropped for the zero start if the error rose)."""
+        if initial_pressure is not None:
+            p0 = np.ascontiguousarray(initial_pressure, np.float32).reshape(-1)
+            if self.L.orc_set_initial_pressure(self.h, _f(p0), p0.size) != 0:
+                raise ValueError("initial_pressure must hold one value per particle")
         st = abi.LspStepStats()
         self.L.orc_step(self.h, dt, ctypes.byref(st))
         return st

@@ -204,6 +204,9 @@ struct SimBase {
 	std::vector<Collider> colliders;
 	std::vector<int64_t> nbrOffsets;
 	std::vector<int32_t> nbrIndex;
+	// Pressure that replaces iteration 0's correction in the next step only (the device's
+	// learned warm start, store_guess in mlp_tc.cu); empty: the reference's zero start.
+	std::vector<float> warmPressure;
 	virtual int64_t count() const = 0;
 	virtual void add(const float* xyz, const float* vel, int64_t n) = 0;
 	virtual int step(float dt, lsp_step_stats* st) = 0;
@@ -442,6 +445,15 @@ struct Sim : SimBase {
 
 	// PCISPHSolver::accumulatePressureForces, CPU branch (PCISPHSolver.cpp:50-170), with the
 	// optional minimum iteration count and the optional velocity keep (both off by default).
+	//
+	// With a warm pressure (warmPressure, caller order) the step follows the device's learned
+	// warm start, which has no counterpart in the reference: iteration 0 predicts from zero
+	// pressure force as :58-62 start it, measures the density error, and then takes the given
+	// pressure instead of its own correction delta * error (:117-125); the loop goes on from
+	// there. The guess is checked once, at iteration 1: if the maximum density error rose
+	// above iteration 0's, the step restarts from the reference's zero start (p = 0, F_p = 0)
+	// and continues exactly as the reference would. A warm step never exits at iteration 0.
+	// `iterations` counts every pass, the rejected ones included.
 	void pcisphPressureForces(T dt, lsp_step_stats* st)
 	{
 		const int64_t N = count();
@@ -453,9 +465,12 @@ struct Sim : SimBase {
 		int it = 0;
 		T ratio = 0;
 		bool converged = false;
+		const bool warm = (int64_t)warmPressure.size() == N && N > 0;
+		bool rejected = false;
+		T maxErr0 = 0;
 		for (int k = 0; k < maxIt; k++)
 		{
-			it = k + 1;
+			it++;
 			// Predict velocity and position (:67-81).
 #pragma omp parallel for schedule(static)
 			for (int64_t i = 0; i < N; i++)
@@ -491,6 +506,7 @@ struct Sim : SimBase {
 				prho[i] = pd;
 				err[i] = er;
 				pres[i] = pres[i] + pp;
+				if (warm && !rejected && k == 0) pres[i] = (T)warmPressure[i];
 			}
 			// Pressure force at the prediction (:129-150); prefactor uses the current density.
 #pragma omp parallel for schedule(static)
@@ -513,9 +529,20 @@ struct Sim : SimBase {
 			// Max density error and the exit test (:152-162).
 			T maxErr = 0;
 			for (int64_t i = 0; i < N; i++) maxErr = std::max(maxErr, (T)std::fabs(err[i]));
+			if (warm && !rejected && k == 1 && maxErr > maxErr0)
+			{
+				// The guess raised the error: the reference's zero start from here on (this
+				// iteration's pressure force is discarded; iteration 0 ignores F_p).
+				rejected = true;
+				for (int64_t i = 0; i < N; i++) { pres[i] = 0; pF[i] = V3<T>(); }
+				k = -1;
+				continue;
+			}
+			if (k == 0) maxErr0 = maxErr;
 			ratio = maxErr / rho0;
 			converged = std::fabs(ratio) < (T)p.pci_eta;
-			if (converged && it >= minIt) break;
+			const bool unverified = warm && !rejected && k == 0;
+			if (converged && k + 1 >= minIt && !unverified) break;
 		}
 		for (int64_t i = 0; i < N; i++) F[i] += pF[i];
 		if (st)
@@ -523,7 +550,10 @@ struct Sim : SimBase {
 			st->iterations = it;
 			st->converged = converged ? 1 : 0;
 			st->max_density_error_ratio = (double)ratio;
+			st->warm_start_tried = warm ? 1 : 0;
+			st->warm_start_used = (warm && !rejected) ? 1 : 0;
 		}
+		warmPressure.clear();
 	}
 
 	// SPHParticle::integrate (SPHParticle.cpp:30-44), per particle.
@@ -681,6 +711,13 @@ int orc_update_sphere(void* h, int index, const float center[3], float radius)
 
 int64_t orc_count(void* h) { return ((SimBase*)h)->count(); }
 int orc_step(void* h, float dt, lsp_step_stats* st) { return ((SimBase*)h)->step(dt, st); }
+int orc_set_initial_pressure(void* h, const float* pressure, int64_t n)
+{
+	SimBase* s = (SimBase*)h;
+	if (n != s->count() || (n > 0 && !pressure)) return -1;
+	s->warmPressure.assign(pressure, pressure + n);
+	return 0;
+}
 int orc_get(void* h, int field, float* out) { return ((SimBase*)h)->get(field, out); }
 int orc_get_f64(void* h, int field, double* out) { return ((SimBase*)h)->getd(field, out); }
 int orc_set_state(void* h, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first)

@@ -28,6 +28,10 @@ int orc_update_box(void* h, int index, const float center[3], const float half_e
 int orc_update_sphere(void* h, int index, const float center[3], float radius);
 int64_t orc_count(void* h);
 int orc_step(void* h, float dt, lsp_step_stats* stats);
+// Next step only: iteration 0 takes this pressure (caller order, n = particle count) in
+// place of its own correction, as the device's learned warm start does; checked at
+// iteration 1 and dropped for the zero start if the maximum density error rose.
+int orc_set_initial_pressure(void* h, const float* pressure, int64_t n);
 int orc_get(void* h, int field, float* out);
 int orc_get_f64(void* h, int field, double* out);
 int orc_set_state(void* h, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first);

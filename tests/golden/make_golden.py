@@ -58,6 +58,9 @@ def generate(kind):
 
 
 if __name__ == "__main__":
-    O.build(ref_dir=os.environ.get("REF_DIR", "/root/reference"))
+    ref_dir = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF_DIR")
+    if not ref_dir:
+        sys.exit("usage: make_golden.py REF_DIR (the reference checkout; or set REF_DIR)")
+    O.build(ref_dir=ref_dir)
     for k in ("sph", "pcisph"):
         print(generate(k), os.path.getsize(os.path.join(HERE, f"{k}_small.npz")))

@@ -42,27 +42,35 @@ def test_static_gradient_matches_allocating_entry_point():
     s.mlp_set_weights(w)
     fp = ctypes.POINTER(ctypes.c_float)
     dev = torch.device("cuda", torch.cuda.current_device())
-    for call, (n, seed) in enumerate([(5000, 11), (777, 12)]):
+    cases = [(5000, 11), (777, 12)]
+    refs, bufs = [], []
+    for n, seed in cases:
         x, t = _batch(n, seed)
         # Reference: the allocating entry point on host arrays.
         g_ref = np.empty(abi.MLP_PARAMS, np.float32)
         l_ref = ctypes.c_float()
         s._call("lsp_mlp_gradient", x.ctypes.data_as(fp), t.ctypes.data_as(fp), n, g_ref.ctypes.data_as(fp),
                 ctypes.byref(l_ref))
-        # The allocation-free entry point on device buffers owned by the caller.
-        dx = torch.from_numpy(x).to(dev)
-        dt = torch.from_numpy(t).to(dev)
-        dg = torch.full((abi.MLP_PARAMS,), float("nan"), dtype=torch.float32, device=dev)
-        dl = torch.full((1,), float("nan"), dtype=torch.float32, device=dev)
-        torch.cuda.synchronize()
+        refs.append((g_ref, l_ref.value))
+        # Device buffers owned by the caller, all created before the allocation-free calls.
+        bufs.append((torch.from_numpy(x).to(dev), torch.from_numpy(t).to(dev),
+                     torch.full((abi.MLP_PARAMS,), float("nan"), dtype=torch.float32, device=dev),
+                     torch.full((1,), float("nan"), dtype=torch.float32, device=dev)))
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(dev)[0]
+    for call, ((n, _), (dx, dt, dg, dl)) in enumerate(zip(cases, bufs)):
         rc = lib.lsp_mlp_gradient_static(s._h, dx.data_ptr(), dt.data_ptr(), n, dg.data_ptr(), dl.data_ptr())
         assert rc == abi.LSP_OK, lib.lsp_last_error()
         s.synchronize()
+    # Nothing was allocated on the device by the two calls (the scratch was set up when the
+    # solver was created).
+    assert torch.cuda.mem_get_info(dev)[0] == free_before
+    for call, ((g_ref, l_ref), (dx, dt, dg, dl)) in enumerate(zip(refs, bufs)):
         g = dg.cpu().numpy()
         loss = float(dl.cpu().numpy()[0])
         rel = np.linalg.norm(g - g_ref) / np.linalg.norm(g_ref)
         assert rel <= 1e-4, (call, rel)
-        assert abs(loss - l_ref.value) <= 1e-5 * abs(l_ref.value), (call, loss, l_ref.value)
+        assert abs(loss - l_ref) <= 1e-5 * abs(l_ref), (call, loss, l_ref)
     # Sizes beyond the fixed scratch are refused with a clear error, and host buffers too.
     rc = lib.lsp_mlp_gradient_static(s._h, dx.data_ptr(), dt.data_ptr(), (1 << 24) + 1, dg.data_ptr(),
                                      dl.data_ptr())
@@ -70,4 +78,11 @@ def test_static_gradient_matches_allocating_entry_point():
     host = np.zeros(8 * 16, np.float32)
     rc = lib.lsp_mlp_gradient_static(s._h, host.ctypes.data, dt.data_ptr(), 16, dg.data_ptr(), dl.data_ptr())
     assert rc == abi.LSP_ERR_INVALID
+    if torch.cuda.device_count() > 1:
+        # A buffer on another GPU is refused before anything is launched (the pointer is
+        # only inspected, never read).
+        other = (torch.cuda.current_device() + 1) % torch.cuda.device_count()
+        far = torch.zeros(8 * 16, dtype=torch.float32, device=torch.device("cuda", other))
+        rc = lib.lsp_mlp_gradient_static(s._h, far.data_ptr(), dt.data_ptr(), 16, dg.data_ptr(), dl.data_ptr())
+        assert rc == abi.LSP_ERR_INVALID and b"solver's GPU" in lib.lsp_last_error()
     s.close()
