@@ -105,6 +105,7 @@ def _orc_lib():
             "orc_count": (c_int64, [V]),
             "orc_step": (c_int, [V, c_float, POINTER(abi.LspStepStats)]),
             "orc_set_initial_pressure": (c_int, [V, _fp, c_int64]),
+            "orc_set_delta_override": (c_int, [V, c_double]),
             "orc_get": (c_int, [V, c_int, _fp]), "orc_get_f64": (c_int, [V, c_int, POINTER(c_double)]),
             "orc_set_state": (c_int, [V, _fp, _fp, _fp, _fp, _i32p]),
             "orc_mass": (c_float, [V]), "orc_kernel_radius": (c_float, [V]), "orc_delta": (c_float, [V, c_float]),
@@ -270,6 +271,10 @@ class OracleSolver:
         st = abi.LspStepStats()
         self.L.orc_step(self.h, dt, ctypes.byref(st))
         return st
+
+    def set_delta(self, delta):
+        """Use this PCISPH pressure scaling instead of the derived one (None: derive it)."""
+        self.L.orc_set_delta_override(self.h, float(delta) if delta else 0.0)
 
     def get(self, field, fp64=False):
         shape = (self.n, 3) if field in abi.VECTOR_FIELDS else (self.n,)

@@ -207,6 +207,11 @@ struct SimBase {
 	// Pressure that replaces iteration 0's correction in the next step only (the device's
 	// learned warm start, store_guess in mlp_tc.cu); empty: the reference's zero start.
 	std::vector<float> warmPressure;
+	// When > 0, the PCISPH pressure scaling delta used instead of calcDelta's. The FP64
+	// instantiation takes the FP32 run's delta (and mass, via mass_override) to isolate the
+	// per-step rounding: both constants are sums over a lattice whose distances fall exactly
+	// on table-slot boundaries, so FP32 and FP64 truncate some of them to different slots.
+	double deltaOverride = 0;
 	virtual int64_t count() const = 0;
 	virtual void add(const float* xyz, const float* vel, int64_t n) = 0;
 	virtual int step(float dt, lsp_step_stats* st) = 0;
@@ -457,7 +462,7 @@ struct Sim : SimBase {
 	void pcisphPressureForces(T dt, lsp_step_stats* st)
 	{
 		const int64_t N = count();
-		const T delta = calcDelta(dt);
+		const T delta = deltaOverride > 0 ? (T)deltaOverride : calcDelta(dt);
 		const T rho0 = (T)p.rest_density;
 		const T neg = (T)p.negative_pressure_factor;
 		for (int64_t i = 0; i < N; i++) { pres[i] = 0; pF[i] = V3<T>(); }
@@ -711,6 +716,11 @@ int orc_update_sphere(void* h, int index, const float center[3], float radius)
 
 int64_t orc_count(void* h) { return ((SimBase*)h)->count(); }
 int orc_step(void* h, float dt, lsp_step_stats* st) { return ((SimBase*)h)->step(dt, st); }
+int orc_set_delta_override(void* h, double delta)
+{
+	((SimBase*)h)->deltaOverride = delta;
+	return 0;
+}
 int orc_set_initial_pressure(void* h, const float* pressure, int64_t n)
 {
 	SimBase* s = (SimBase*)h;

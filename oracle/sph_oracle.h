@@ -32,6 +32,8 @@ int orc_step(void* h, float dt, lsp_step_stats* stats);
 // place of its own correction, as the device's learned warm start does; checked at
 // iteration 1 and dropped for the zero start if the maximum density error rose.
 int orc_set_initial_pressure(void* h, const float* pressure, int64_t n);
+// PCISPH pressure scaling used instead of the derived one (0: derive it, the default).
+int orc_set_delta_override(void* h, double delta);
 int orc_get(void* h, int field, float* out);
 int orc_get_f64(void* h, int field, double* out);
 int orc_set_state(void* h, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first);

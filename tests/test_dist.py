@@ -54,3 +54,21 @@ def test_two_rank_gloo_replicas(tmp_path):
         assert r["t_max"] == 15.0                    # max over ranks, not the local time
         assert r["total"] == 2 * 3 * r["n"]          # every rank's updates are counted
         assert r["firsts"][0] != r["firsts"][1]      # replicas are different seeded scenes
+
+
+def test_bench_cli_launches_its_own_ranks():
+    """`python bench.py --gpus 2` outside torchrun starts two ranks itself; --dry-run runs the
+    replica path on CPU oracle samples over gloo. One line, from rank 0, with n_gpus 2 and the
+    aggregate of both ranks."""
+    import json
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE")}
+    r = subprocess.run([sys.executable, "bench.py", "--gpus", "2", "--dry-run", "--steps", "2", "--warmup", "1",
+                        "--workload", "dam_break_pcisph"], cwd=ROOT, env=env, capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["n_gpus"] == 2 and d["dry_run"] is True and d["config"]["parallelism"] == "replicas x2"
+    assert abs(d["value"] - 2 * d["particles_per_rank"] * d["steps"] / (d["ms_per_step"] * d["steps"] / 1e3)) \
+        <= 1e-6 * d["value"]

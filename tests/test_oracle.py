@@ -4,6 +4,8 @@ oracle/_ref/libref_sph.so is the reference's own LiquidPhysics/src, compiled
 unmodified (oracle/Makefile). oracle/liblsp_oracle.so is the project's restatement.
 They must agree bit for bit on every field, every step, and on the neighbour lists.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -82,6 +84,64 @@ def test_fp64_oracle_bounds_fp32_error(oracle_mod):
     assert d.max() / rho0 < 1e-5
     x = np.abs(o32.get(abi.FIELD_POSITION).astype(np.float64) - o64.get(abi.FIELD_POSITION, fp64=True))
     assert x.max() < 1e-6
+
+
+def test_fp64_error_at_scale(oracle_mod, capsys):
+    """States the FP32 error against the FP64 restatement at 102,400 particles (PCISPH dam
+    break, s = 0.00625) over three steps from one injected state (after a 20-step FP32
+    lead-in), six iterations per step so both run the same loop. The FP64 run takes the FP32
+    mass and delta: both are sums over a lattice whose distances fall exactly on table-slot
+    boundaries, so FP32 and FP64 would otherwise derive constants 0.2 % apart.
+
+    Measured (and asserted below for the first step): start-of-step density within 6.4e-8 of
+    rho0 at the median and 3.0e-7 at the 99.9th percentile, the FP32 rounding; its maximum
+    is 3.3e-4, where a pair's distance straddles a table-slot boundary and the reference's
+    truncating lookup (SPHKernel.cpp:13-22) moves one table step. Through the predict-correct
+    loop those differences reach the pressure (median 1.4e-6, 99.9th percentile 1.3e-2 of the
+    largest pressure) and the velocity (median 3.7e-4 of the largest speed); over the next
+    steps they grow, as perturbations of a particle flow do (density median 2e-4 by step 3)."""
+    import copy
+    oracle_mod.set_threads(os.cpu_count() or 1)
+    sc = scenes.dam_break_pcisph(seed=2, counts=(40, 64, 40), s=0.00625)
+    o = oracle_mod.OracleSolver(sc)
+    for _ in range(20):
+        o.step(sc.dt)
+    state = [o.get(f) for f in (abi.FIELD_POSITION, abi.FIELD_VELOCITY, abi.FIELD_HALF_VELOCITY,
+                                abi.FIELD_OLD_HALF_VELOCITY)]
+    first = o.get(abi.FIELD_FIRST_STEP).astype(np.int32)
+    m32, d32 = o.mass(), o.delta(sc.dt)
+    o.close()
+    p = sc.params
+    p.pci_min_iterations = p.pci_max_iterations = 6
+    p64 = copy.copy(p)
+    p64.mass_override = m32
+    a = oracle_mod.OracleSolver(sc, params=p)
+    b = oracle_mod.OracleSolver(sc, fp64=True, params=p64)
+    b.set_delta(d32)
+    a.set_state(*state, first)
+    b.set_state(*state, first)
+    qs = (0.5, 0.999, 1.0)
+    rows = []
+    for step in range(3):
+        a.step(sc.dt)
+        b.step(sc.dt)
+        rho = np.abs(a.get(abi.FIELD_DENSITY).astype(np.float64) - b.get(abi.FIELD_DENSITY, fp64=True))
+        p64v = b.get(abi.FIELD_PRESSURE, fp64=True)
+        pr = np.abs(a.get(abi.FIELD_PRESSURE).astype(np.float64) - p64v) / np.abs(p64v).max()
+        v64 = b.get(abi.FIELD_VELOCITY, fp64=True)
+        vv = np.linalg.norm(a.get(abi.FIELD_VELOCITY).astype(np.float64) - v64, axis=1)
+        rows.append((np.quantile(rho / p.rest_density, qs), np.quantile(pr, qs),
+                     np.quantile(vv / np.linalg.norm(v64, axis=1).max(), qs)))
+    a.close()
+    b.close()
+    with capsys.disabled():
+        for step, (r, q, v) in enumerate(rows):
+            print(f"\nFP32 vs FP64, 102,400 particles, step {step + 1} (median / 99.9 % / max): density "
+                  f"{r[0]:.1e} {r[1]:.1e} {r[2]:.1e} of rho0; pressure {q[0]:.1e} {q[1]:.1e} {q[2]:.1e} "
+                  f"of max |p|; velocity {v[0]:.1e} {v[1]:.1e} {v[2]:.1e} of max |v|")
+    r, q, v = rows[0]
+    assert r[0] < 2e-7 and r[1] < 1e-6 and r[2] < 1e-3
+    assert q[0] < 1e-5 and q[2] < 5e-2 and v[0] < 1e-3 and v[2] < 5e-2
 
 
 def test_min_iteration_floor(oracle_mod):

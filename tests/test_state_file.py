@@ -90,3 +90,59 @@ def test_saved_run_resumes_bit_identically(tmp_path, warm):
             assert np.array_equal(a.read(fld).view(np.uint32), b.read(fld).view(np.uint32)), (step, fld)
     a.close()
     b.close()
+
+
+def read_file(path):
+    """The state file's contents, parsed on the CPU from the layout documented in
+    csrc/state_io.cpp: (flags, seed, params, domain, colliders, x, v, v_half, v_half_old, first)."""
+    b = path.read_bytes()
+    assert b[:8] == MAGIC
+    version, flags, seed, n, ncol, psize = struct.unpack_from("<IIQqiI", b, 8)
+    assert version == 1 and psize == ctypes.sizeof(abi.LspParams)
+    off = 8 + struct.calcsize("<IIQqiI")
+    params = abi.LspParams.from_buffer_copy(b[off:off + psize])
+    off += psize
+    lo_hi = struct.unpack_from("<6f", b, off)
+    off += 24
+    cols = []
+    for _ in range(ncol):
+        sphere, boundary, *rest = struct.unpack_from("<2i7f", b, off)
+        off += struct.calcsize("<2i7f")
+        c, h, r = rest[0:3], rest[3:6], rest[6]
+        cols.append(scenes.Collider("sphere", tuple(c), r, bool(boundary)) if sphere
+                    else scenes.Collider("box", tuple(c), tuple(h), bool(boundary)))
+    arrs = []
+    for _ in range(4):
+        arrs.append(np.frombuffer(b, np.float32, 3 * n, off).reshape(n, 3).copy())
+        off += 12 * n
+    first = np.frombuffer(b, np.int32, n, off).copy()
+    return flags, seed, params, (lo_hi[:3], lo_hi[3:]), cols, arrs, first
+
+
+@pytest.mark.gpu
+def test_resumed_run_matches_the_oracle_from_the_file(tmp_path):
+    """A state file saved mid-run is parsed here on the CPU; the oracle starts from its
+    caller-order state, parameters and colliders, the library from lsp_load_state, and both
+    take three steps: 0 ulp on every field, equal iteration counts."""
+    from oracle import oracle as O
+    sc = scenes.dam_break_pcisph(seed=6, counts=(14, 22, 14), s=0.02)
+    a = from_scene(sc)
+    for _ in range(5):
+        a.update(sc.dt)
+    f = tmp_path / "mid.lspstate"
+    a.save_state(f, seed=6)
+    a.close()
+    flags, seed, params, domain, cols, (x, v, h, old), first = read_file(f)
+    assert seed == 6 and x.shape == (sc.n, 3) and first.max() == 0
+    b = PCISPHSolver()
+    b.load_state(f)
+    file_scene = scenes.Scene("from_file", params, x, v, cols, sc.dt, 3, domain=domain)
+    o = O.OracleSolver(file_scene)
+    o.set_state(x, v, h, old, first)
+    for step in range(3):
+        sb, so = b.update(sc.dt), o.step(sc.dt)
+        assert sb.iterations == so.iterations, step
+        for fld in FIELDS:
+            assert np.array_equal(b.read(fld).view(np.uint32), o.get(fld).view(np.uint32)), (step, fld)
+    b.close()
+    o.close()
