@@ -204,6 +204,11 @@ int lsp_mlp_set_weights(lsp_solver* s, const float* w, int n);
 int lsp_mlp_get_weights(lsp_solver* s, float* w, int n);
 /* Records the 8 features of every particle at iteration 0 of each PCISPH step. */
 int lsp_mlp_record(lsp_solver* s, int enable);
+/* Sets params.warm_start (LSP_WARM_ZERO / LSP_WARM_MLP / LSP_WARM_AUTO) alone, without the
+ * table rebuild of lsp_set_params, for callers that switch the warm start between steps
+ * (online retraining with the zero start as fallback). LSP_WARM_AUTO restarts from the zero
+ * start. No counterpart in the reference. */
+int lsp_set_warm_start(lsp_solver* s, int mode);
 /* Training loss 1/(2n) sum w r^2, r = guess - target, w = over_weight when r > 0
  * (default 1, plain MSE). PCISPH with a zero negative-pressure factor only adds pressure
  * within a step, so over-estimates cost iterations that under-estimates do not. */
@@ -240,7 +245,7 @@ int lsp_timer_mark(lsp_solver* s, int slot);
 int lsp_timer_elapsed(lsp_solver* s, int slot_a, int slot_b, float* ms);
 /* Per-kernel-class device time: with profiling on, every launch is bracketed by events on
  * the solver's stream. read: ms[k] and launches[k] for k < LSP_PROF_COUNT. */
-#define LSP_PROF_GRID_SORT     0   /* cell keys, histogram, scan, scatter, rank + gather */
+#define LSP_PROF_GRID_SORT     0   /* cell keys and histogram (batches: the whole grid build) */
 #define LSP_PROF_NEIGHBORS     1
 #define LSP_PROF_DENSITY       2
 #define LSP_PROF_NONPRESSURE   3
@@ -251,7 +256,10 @@ int lsp_timer_elapsed(lsp_solver* s, int slot_a, int slot_b, float* ms);
 #define LSP_PROF_INTEGRATE     8
 #define LSP_PROF_PCI_LOOP      9   /* the persistent predict-correct kernel */
 #define LSP_PROF_WARM_START    10
-#define LSP_PROF_COUNT         11
+#define LSP_PROF_GRID_SCAN     11  /* scan of the histogram into the dense cell table */
+#define LSP_PROF_GRID_SCATTER  12  /* particle -> cell start + slot */
+#define LSP_PROF_GRID_GATHER   13  /* rank inside each cell and gather of the persistent state */
+#define LSP_PROF_COUNT         14
 int lsp_profile(lsp_solver* s, int enable);
 int lsp_profile_read(lsp_solver* s, double* ms, int64_t* launches, int capacity);
 /* Kernels this solver has launched since creation. */

@@ -50,8 +50,9 @@ FIELD_SPEED_SQUARED = 13
 VECTOR_FIELDS = {FIELD_POSITION, FIELD_VELOCITY, FIELD_HALF_VELOCITY, FIELD_PRED_POSITION,
                  FIELD_PRED_HALF_VELOCITY, FIELD_PRED_PRESSURE_FORCE, FIELD_OLD_HALF_VELOCITY}
 
-PROF_NAMES = ["grid_sort", "neighbors", "density", "nonpressure", "sph_pressure", "pci_predict",
-              "pci_density", "pci_force", "integrate_collide", "pci_loop", "warm_start"]
+PROF_NAMES = ["grid_keys", "neighbors", "density", "nonpressure", "sph_pressure", "pci_predict",
+              "pci_density", "pci_force", "integrate_collide", "pci_loop", "warm_start", "grid_scan",
+              "grid_scatter", "grid_gather"]
 
 MLP_PARAMS = 1377
 MLP_FEATURES = 8
@@ -230,6 +231,7 @@ def _declare(lib):
         "lsp_mlp_set_weights": (c_int, [S, fp, c_int]),
         "lsp_mlp_get_weights": (c_int, [S, fp, c_int]),
         "lsp_mlp_record": (c_int, [S, c_int]),
+        "lsp_set_warm_start": (c_int, [S, c_int]),
         "lsp_mlp_set_loss_asymmetry": (c_int, [S, c_float]),
         "lsp_mlp_train": (c_int, [S, c_int, c_int, c_float, ctypes.c_uint64, fp]),
         "lsp_mlp_forward": (c_int, [S, fp, c_int64, fp]),

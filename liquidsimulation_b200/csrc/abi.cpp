@@ -296,6 +296,10 @@ int lsp_mlp_record(lsp_solver* s, int enable)
 {
     return lsp::guard([&] { E(s).mlp_record(enable != 0); });
 }
+int lsp_set_warm_start(lsp_solver* s, int mode)
+{
+    return lsp::guard([&] { E(s).set_warm_start(mode); });
+}
 int lsp_mlp_set_loss_asymmetry(lsp_solver* s, float over_weight)
 {
     return lsp::guard([&] { E(s).mlp_set_loss_asymmetry(over_weight); });

@@ -201,6 +201,15 @@ void Engine::set_params(const lsp_params& p)
     if (geometry) nbr_cap_ = 0;  // re-estimate the list capacity for the new h
 }
 
+void Engine::set_warm_start(int mode)
+{
+    lsp_params p = prm_;
+    p.warm_start = mode;
+    validate_params(p);
+    prm_.warm_start = mode;
+    auto_on_ = false;
+}
+
 static int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 void Engine::ensure_capacity(int64_t n)
@@ -740,7 +749,10 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
         // The neighbour build also sums the start-of-step density (k_neighbors_density).
         g.tables = tables_.p; g.rho = rho_.p; g.pres = pres_.p;
-        timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_sort(g, stream_); });
+        timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_keys(g, stream_); });
+        timed(LSP_PROF_GRID_SCAN, [&] { return launch_grid_scan(g, stream_); });
+        timed(LSP_PROF_GRID_SCATTER, [&] { return launch_grid_scatter(g, stream_); });
+        timed(LSP_PROF_GRID_GATHER, [&] { return launch_grid_gather(g, stream_); });
         timed(LSP_PROF_NEIGHBORS, [&] { return launch_neighbors(g, stream_); });
         cur_ = 1 - cur_;
         StepBuffers b = buffers();

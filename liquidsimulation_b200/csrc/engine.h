@@ -49,6 +49,8 @@ public:
     ~Engine();
 
     void set_params(const lsp_params& p);
+    // params.warm_start alone (no table rebuild); LSP_WARM_AUTO starts from the zero start.
+    void set_warm_start(int mode);
     const lsp_params& params() const { return prm_; }
     float mass() const { return hk_.mass; }
     float kernel_radius() const { return hk_.h; }

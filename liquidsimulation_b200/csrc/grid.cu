@@ -210,6 +210,40 @@ __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
 
 static inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+int launch_grid_keys(const GridBuildArgs& a, cudaStream_t s)
+{
+    if (a.P.n <= 0) return 0;
+    k_keys_hist<<<blocks_for(a.P.n, 256), 256, 0, s>>>(a.P, a.pos_in, a.key, a.slot, a.hist, a.status);
+    return 1;
+}
+
+int launch_grid_scan(const GridBuildArgs& a, cudaStream_t s)
+{
+    const int64_t n = (int64_t)a.P.cells + 1;
+    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
+    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
+    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
+    return 3;
+}
+
+int launch_grid_scatter(const GridBuildArgs& a, cudaStream_t s)
+{
+    if (a.P.n <= 0) return 0;
+    k_scatter<<<blocks_for(a.P.n, 256), 256, 0, s>>>(a.P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
+    return 1;
+}
+
+int launch_grid_gather(const GridBuildArgs& a, cudaStream_t s)
+{
+    if (a.P.n <= 0) return 0;
+    k_rank_gather<<<blocks_for(a.P.n, 256), 256, 0, s>>>(a.P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,
+                                                         a.half_in, a.old_in, a.pos_out, a.vel_out, a.half_out,
+                                                         a.old_out, a.slot_of_id, a.sorted_key, a.status,
+                                                         a.hist_in, a.hist_out);
+    return 1;
+}
+
 int launch_grid_order(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;

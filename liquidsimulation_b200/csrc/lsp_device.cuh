@@ -51,7 +51,8 @@ struct DevStatus {
     uint32_t timeout_site;
     float last_ratio;
     int32_t last_k;             // logical index of the loop's last iteration (persistent loop)
-    uint32_t pad[4];
+    uint32_t div_unsafe;        // a predicted position left exact_div_safe's range this step
+    uint32_t pad[3];
 };
 
 struct DevParams {
@@ -116,6 +117,40 @@ __device__ __forceinline__ void normalize(V3& a)
     if (m > 0.f) a *= (1.f / m);
 }
 __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+
+// Correctly rounded quotients a / d from one reciprocal per denominator, after Markstein's
+// method (P. Markstein, "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Develop. 34(1), 1990; "IA-64 and Elementary Functions", 2000,
+// ch. 8): one Newton-Raphson step with fused multiply-adds turns the hardware's approximate
+// reciprocal (within one ulp) into RN(1 / d), and with y = RN(1 / d) and q0 = RN(a * y),
+// within one ulp of a / d, the residual r = a - d * q0 is exact and RN(q0 + r * y) is
+// RN(a / d). recip_rn is checked against the IEEE reciprocal for every positive normal
+// float and div_by against IEEE division on billions of pairs
+// (tests/cpp/exact_div_check.cu). The theorem needs every value normal: callers use them
+// only where 2^-99 <= d <= 2^27 and a is 0 or 2^-99 <= |a| <= d (exact_div_safe). A zero
+// numerator gives a zero of either sign, which adds to a sum started at +0 like the IEEE
+// quotient's zero does.
+__device__ __forceinline__ float recip_rn(float d)
+{
+    float y0;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(d));
+    const float e = __fmaf_rn(-d, y0, 1.f);
+    return __fmaf_rn(e, y0, y0);
+}
+__device__ __forceinline__ float div_by(float a, float d, float y)
+{
+    const float q0 = __fmul_rn(a, y);
+    const float r = __fmaf_rn(-d, q0, a);
+    return __fmaf_rn(r, y, q0);
+}
+// A coordinate with which every pair difference, and its quotient by the pair distance,
+// stays where div_by is exact: 0, or 2^-76 <= |c| <= 2^26 (nonzero differences of such
+// floats are at least 2^-99 and distances at most 2^28).
+__device__ __forceinline__ bool exact_div_safe(float c)
+{
+    const float a = fabsf(c);
+    return a == 0.f || (a >= 0x1p-76f && a <= 0x1p26f);
+}
 
 // SPHKernel::get*Weight (SPHKernel.cpp:13-44): zero at or beyond h, else the table
 // entry at trunc(d / step), with d / step rounded as IEEE division rounds it.

@@ -81,6 +81,12 @@ int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
 // the cell table, scatter, rank by caller id and gather of a.P.n particles.
 int launch_grid_order(const GridBuildArgs& a, cudaStream_t s);
 int launch_neighbors(const GridBuildArgs& a, cudaStream_t s);
+// The grid build's four passes one by one (launch_grid_sort = all four in order): cell keys
+// and histogram, scan into the cell table, scatter, rank + gather.
+int launch_grid_keys(const GridBuildArgs& a, cudaStream_t s);
+int launch_grid_scan(const GridBuildArgs& a, cudaStream_t s);
+int launch_grid_scatter(const GridBuildArgs& a, cudaStream_t s);
+int launch_grid_gather(const GridBuildArgs& a, cudaStream_t s);
 
 // With b.gradrho set, also stores |grad rho| (a warm-start feature).
 void launch_nonpressure(const DevParams& P, const StepBuffers& b, cudaStream_t s);

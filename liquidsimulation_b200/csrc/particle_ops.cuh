@@ -299,6 +299,9 @@ __device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBu
     V3 ph = hv + acc * P.dt;
     V3 px = v3(b.pos[i]) + ph * P.dt;
     collide_all(b.colliders + P.coll_off, P.ncoll, px, ph, P);
+    // The force pass divides by pair distances with div_by while every prediction of the
+    // step stays in its exact range; one position outside switches it to IEEE division.
+    if (!(exact_div_safe(px.x) && exact_div_safe(px.y) && exact_div_safe(px.z))) atomicOr(&b.status->div_unsafe, 1u);
     ppos[i] = f4(px, 0.f);
     b.phalf[i] = f4(ph, 0.f);
     if (iteration == 0 && !P.keep_initial_velocity) {
@@ -338,9 +341,13 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 }
 
 // PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
-// reference recomputes per pair; the prefactor uses the current density rho_i.
-__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
-                                              const float* TH, int i, const float4* ppos)
+// reference recomputes per pair; the prefactor uses the current density rho_i. The pair
+// direction (x_i - x_j) / d is three IEEE quotients; with kExactDiv they come from one
+// reciprocal of d (recip_rn, div_by), the same bits for the predicted positions the step's
+// predict passes found safe (DevStatus::div_unsafe clear).
+template <bool kExactDiv>
+__device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuffers& b, const float* SDW,
+                                               const float* TH, int i, const float4* ppos)
 {
     const float4 pi4 = ppos[i];
     const V3 xi = v3(pi4);
@@ -354,12 +361,24 @@ __device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuff
                              // (the squares are equal), so one difference serves both.
                              const V3 dq = xi - v3(pj4);
                              float d = mag(dq);
-                             V3 dir = dq / d;
+                             V3 dir;
+                             if (kExactDiv) {
+                                 const float y = recip_rn(d);
+                                 dir = v3(div_by(dq.x, d, y), div_by(dq.y, d, y), div_by(dq.z, d, y));
+                             } else {
+                                 dir = dq / d;
+                             }
                              pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
                          });
     pf *= -(P.mass * b.rho[i]);
     if (isnan(pf.x)) pf = v3(0.f, 0.f, 0.f);
     b.pforce[i] = f4(pf, 0.f);
+}
+__device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
+                                              const float* TH, int i, const float4* ppos)
+{
+    if (*(const volatile uint32_t*)&b.status->div_unsafe == 0u) pci_force_walk<true>(P, b, SDW, TH, i, ppos);
+    else pci_force_walk<false>(P, b, SDW, TH, i, ppos);
 }
 
 }  // namespace lsp

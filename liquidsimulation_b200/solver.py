@@ -281,7 +281,16 @@ class SPHSolver:
         return out
 
     def set_warm_start(self, mode: int):
-        self.set_params(warm_start=int(mode))
+        """params.warm_start alone (lsp_set_warm_start: no table rebuild)."""
+        self._call("lsp_set_warm_start", int(mode))
+
+    def grid_cells(self) -> int:
+        """Cells of the grid box of the last step (the dense cell table has one entry more)."""
+        dims = np.empty(3, np.int32)
+        org = np.empty(3, np.int32)
+        cells = c_int64()
+        self._call("lsp_grid_info", _ptr(dims, POINTER(c_int32)), _ptr(org, POINTER(c_int32)), byref(cells))
+        return int(cells.value)
 
     def grid(self):
         """(dims, origin, sorted keys, sorted caller ids, dense cell table) of the last step."""
@@ -320,6 +329,68 @@ class PCISPHSolver(SPHSolver):
     def set_minimum_iteration_floor(self, n: int):
         """Extension: no convergence exit before n iterations (the reference has none)."""
         self.set_params(pci_min_iterations=int(n))
+
+
+class OnlineWarmStart:
+    """Learned warm start retrained online, with the reference's zero start as fallback.
+
+    Drives one PCISPH solver step by step. A training step runs the plain solver (zero
+    initial pressure, PCISPHSolver.cpp:58-62) with its features recorded and, if it met eta,
+    takes `iterations` Adam steps on its final pressures: the first `lead` steps, then every
+    `every`-th step. Every other step starts from the network's guess (LSP_WARM_MLP), once the
+    network has been trained at least once; a warm step that misses eta switches the solver
+    back to the zero start until the next training step (the fallback). The network never
+    trains on warm-started outputs. A scene that grows (particles appended between steps)
+    is handled: features are recorded per step."""
+
+    def __init__(self, solver, every: int = 500, lead: int = 50, iterations: int = 8, batch: int = 65536,
+                 lr: float = 2e-3, loss_asymmetry: float = 4.0):
+        if every < 1 or lead < 0:
+            raise ValueError("every must be >= 1 and lead >= 0")
+        self.s = solver
+        self.every, self.lead, self.iterations, self.batch, self.lr = every, lead, iterations, batch, lr
+        self.k = 0
+        self.trained_steps = 0
+        self.training_steps = 0
+        self.fallback_steps = 0
+        self.warm_steps = 0
+        self._healthy = True
+        solver.mlp_set_loss_asymmetry(loss_asymmetry)
+        solver.set_warm_start(abi.LSP_WARM_ZERO)
+
+    def _mode(self, mode):
+        if self.s.params.warm_start != mode:
+            self.s.set_warm_start(mode)
+
+    def is_training_step(self, k: int) -> bool:
+        return k < self.lead or (k - self.lead) % self.every == self.every - 1
+
+    def update(self, dt: float) -> abi.LspStepStats:
+        k = self.k
+        self.k += 1
+        s = self.s
+        if self.is_training_step(k):
+            self._mode(abi.LSP_WARM_ZERO)
+            s.mlp_record(True)
+            st = s.update(dt)
+            s.mlp_record(False)
+            self.training_steps += 1
+            eta = s.params.pci_eta
+            if st.converged and st.max_density_error_ratio <= eta + 1e-12:
+                s.mlp_train(iterations=self.iterations, batch=self.batch, lr=self.lr, seed=k)
+                self.trained_steps += 1
+            self._healthy = True
+            return st
+        warm = self.trained_steps > 0 and self._healthy
+        self._mode(abi.LSP_WARM_MLP if warm else abi.LSP_WARM_ZERO)
+        st = s.update(dt)
+        if warm:
+            self.warm_steps += 1
+            if not st.converged:
+                self._healthy = False
+        else:
+            self.fallback_steps += 1
+        return st
 
 
 def state_file_info(path: str) -> dict:
