@@ -127,7 +127,7 @@ __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.
 // RN(a / d). recip_rn is checked against the IEEE reciprocal for every positive normal
 // float and div_by against IEEE division on billions of pairs
 // (tests/cpp/exact_div_check.cu). The theorem needs every value normal: callers use them
-// only where 2^-99 <= d <= 2^27 and a is 0 or 2^-99 <= |a| <= d (exact_div_safe). A zero
+// only where 2^-62 <= d <= 2^28 and a is 0 or 2^-62 <= |a| <= d (exact_div_safe). A zero
 // numerator gives a zero of either sign, which adds to a sum started at +0 like the IEEE
 // quotient's zero does.
 __device__ __forceinline__ float recip_rn(float d)
@@ -143,13 +143,28 @@ __device__ __forceinline__ float div_by(float a, float d, float y)
     const float r = __fmaf_rn(-d, q0, a);
     return __fmaf_rn(r, y, q0);
 }
-// A coordinate with which every pair difference, and its quotient by the pair distance,
-// stays where div_by is exact: 0, or 2^-76 <= |c| <= 2^26 (nonzero differences of such
-// floats are at least 2^-99 and distances at most 2^28).
+// The same for the square root: the approximate reciprocal square root and one correction
+// with the exact residual s - g^2 (Markstein's square-root step), equal to the IEEE square
+// root for every normal s (checked for every one, tests/cpp/exact_div_check.cu). s = 0 gives
+// NaN where IEEE gives 0; the force pass only takes it for pairs j != i, where a zero distance
+// makes the direction 0 / 0 = NaN either way.
+__device__ __forceinline__ float sqrt_rn(float s)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
+    const float g = __fmul_rn(s, y);
+    const float h = __fmul_rn(0.5f, y);
+    const float r = __fmaf_rn(-g, g, s);
+    return __fmaf_rn(r, h, g);
+}
+// A coordinate with which every pair difference, its squared length and its quotient by the
+// pair distance stay where sqrt_rn and div_by are exact: 0, or 2^-39 <= |c| <= 2^26 (nonzero
+// differences of such floats are at least 2^-62, their squared lengths at least 2^-124 and at
+// most 3 * 2^54).
 __device__ __forceinline__ bool exact_div_safe(float c)
 {
     const float a = fabsf(c);
-    return a == 0.f || (a >= 0x1p-76f && a <= 0x1p26f);
+    return a == 0.f || (a >= 0x1p-39f && a <= 0x1p26f);
 }
 
 // SPHKernel::get*Weight (SPHKernel.cpp:13-44): zero at or beyond h, else the table

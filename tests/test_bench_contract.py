@@ -28,17 +28,37 @@ def _line(args, timeout):
     return d
 
 
+def _our_config(args):
+    """The config our arm prints for the same arguments (built without a GPU)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    old = sys.argv
+    try:
+        sys.argv = ["bench.py", *args]
+        a = bench.parse()
+    finally:
+        sys.argv = old
+    return bench.line_config(a, 1)
+
+
 def test_reference_arm_line():
-    d = _line(["--impl", "reference", "--steps", "1", "--warmup", "1"], 900)
+    args = ["--impl", "reference", "--steps", "1", "--warmup", "1"]
+    d = _line(args, 900)
     assert d["impl"] == "reference"
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # The same config dict as our arm's line for the same workload, naming the CPU sample.
+    assert d["config"] == _our_config(args) and "sub-scene" in d["config"]["reference_arm"]
+    assert d["iterations_mean"] >= 1 and d["particle_iterations_per_s"] == d["value"] * d["iterations_mean"]
+    port = d["port_same_iteration_rule"]
+    assert port["kind"] == "port" and port["iterations_mean"] >= 3
 
 
 @pytest.mark.gpu
 def test_library_arm_line():
-    d = _line(["--steps", "3", "--warmup", "3", "--train-steps", "5", "--long-steps", "0"], 1200)
+    d = _line(["--steps", "3", "--warmup", "3", "--train-steps", "5", "--long-steps", "0", "--same-steps", "20"],
+              1200)
     assert d["n_gpus"] == 1 and d["steps"] == 3 and d["warmup"] == 3 and d["dtype"] == "f32"
     r = d["roofline"]
     assert r["bound"] in ("hbm", "tensor") and r["unit"] in ("GB/s", "TFLOP/s")
@@ -50,3 +70,11 @@ def test_library_arm_line():
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(c) and c["samples"] > 0
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("reference", "port") and cb["value"] > 0
+    passes = r["passes"]
+    assert {"pci_loop", "neighbors", "nonpressure", "grid_keys", "grid_scan", "grid_scatter",
+            "grid_gather"} <= set(passes)
+    for v in passes.values():
+        assert v["ms_per_step"] > 0 and (v["frac"] is None or 0 < v["frac"] < 2)
+    assert d["config"] == _our_config(["--steps", "3", "--warmup", "3", "--train-steps", "5", "--long-steps", "0"])
+    ss = d["same_state"]
+    assert len(ss) == 2 and all(x["samples"] > 0 for x in ss)
