@@ -143,24 +143,9 @@ __device__ __forceinline__ float div_by(float a, float d, float y)
     const float r = __fmaf_rn(-d, q0, a);
     return __fmaf_rn(r, y, q0);
 }
-// The same for the square root: the approximate reciprocal square root and one correction
-// with the exact residual s - g^2 (Markstein's square-root step), equal to the IEEE square
-// root for every normal s (checked for every one, tests/cpp/exact_div_check.cu). s = 0 gives
-// NaN where IEEE gives 0; the force pass only takes it for pairs j != i, where a zero distance
-// makes the direction 0 / 0 = NaN either way.
-__device__ __forceinline__ float sqrt_rn(float s)
-{
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
-    const float g = __fmul_rn(s, y);
-    const float h = __fmul_rn(0.5f, y);
-    const float r = __fmaf_rn(-g, g, s);
-    return __fmaf_rn(r, h, g);
-}
-// A coordinate with which every pair difference, its squared length and its quotient by the
-// pair distance stay where sqrt_rn and div_by are exact: 0, or 2^-39 <= |c| <= 2^26 (nonzero
-// differences of such floats are at least 2^-62, their squared lengths at least 2^-124 and at
-// most 3 * 2^54).
+// A coordinate with which every pair difference and its quotient by the pair distance stay
+// where div_by is exact: 0, or 2^-39 <= |c| <= 2^26 (nonzero differences of such floats are
+// at least 2^-62 and distances at most 2^28).
 __device__ __forceinline__ bool exact_div_safe(float c)
 {
     const float a = fabsf(c);

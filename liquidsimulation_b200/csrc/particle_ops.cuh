@@ -342,10 +342,9 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 
 // PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
 // reference recomputes per pair; the prefactor uses the current density rho_i. The pair
-// distance is an IEEE square root and the direction (x_i - x_j) / d three IEEE quotients;
-// with kExactDiv they come from sqrt_rn and one reciprocal of d (recip_rn, div_by), the same
-// bits for the predicted positions the step's predict passes found safe
-// (DevStatus::div_unsafe clear).
+// direction (x_i - x_j) / d is three IEEE quotients; with kExactDiv they come from one
+// reciprocal of d (recip_rn, div_by), the same bits for the predicted positions the step's
+// predict passes found safe (DevStatus::div_unsafe clear).
 template <bool kExactDiv>
 __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuffers& b, const float* SDW,
                                                const float* TH, int i, const float4* ppos)
@@ -361,7 +360,7 @@ __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuf
                              // |x_i - x_j| rounds exactly like the reference's |x_j - x_i|
                              // (the squares are equal), so one difference serves both.
                              const V3 dq = xi - v3(pj4);
-                             const float d = kExactDiv ? sqrt_rn(sqmag(dq)) : mag(dq);
+                             const float d = mag(dq);
                              V3 dir;
                              if (kExactDiv) {
                                  const float y = recip_rn(d);
