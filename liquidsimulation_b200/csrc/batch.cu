@@ -95,6 +95,8 @@ __global__ void __launch_bounds__(T) kb_neighbors_density(BatchArgs a, const flo
         if (pr < 0.f) pr *= P.neg;
         rho[i] = r;
         pres[i] = pr;
+        // Batch-wide, like the rest of the non-pressure pass's range checks (k_rank_gather).
+        if (!exact_div_density(r)) atomicOr(&a.st[a.scenes].np_unsafe, 1u);
     }
     record_neighbor_count(P, c, valid, a.st + it.scene);
 }

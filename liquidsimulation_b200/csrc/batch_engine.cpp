@@ -188,9 +188,11 @@ void BatchEngine::build()
     rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap);
     key_.alloc(cap); slot_.alloc(cap); sorted_key_.alloc(cap); tmp_.alloc(cap);
     slot_of_id_.alloc(cap); nbr_count_.alloc(cap);
-    hist_.alloc(cells_ + 1);
-    cell_start_.alloc(cells_ + 1);
-    tile_sums_.alloc((cells_ + 1 + 2047) / 2048 + 1);
+    // The scan reads and writes the histogram and cell table 8 entries at a time: both are
+    // padded to a multiple of 8 with zeros (scan_entries).
+    hist_.alloc(scan_entries(cells_ + 1));
+    cell_start_.alloc(scan_entries(cells_ + 1));
+    tile_sums_.alloc(scan_tiles(cells_ + 1) + 1);
     loop_sync_.alloc(4);
     maxerr_.alloc((size_t)S * mstride_);
     status_.alloc(S + 1);
@@ -201,7 +203,8 @@ void BatchEngine::build()
     CK(cudaMallocHost((void**)&hstatus_, (S + 1) * sizeof(DevStatus)));
     std::memset(hstatus_, 0, (S + 1) * sizeof(DevStatus));
 
-    CK(cudaMemsetAsync(hist_.p, 0, (cells_ + 1) * sizeof(uint32_t), stream_));
+    CK(cudaMemsetAsync(hist_.p, 0, scan_entries(cells_ + 1) * sizeof(uint32_t), stream_));
+    CK(cudaMemsetAsync(cell_start_.p, 0, scan_entries(cells_ + 1) * sizeof(uint32_t), stream_));
     CK(cudaMemsetAsync(cell_start_.p, 0, (cells_ + 1) * sizeof(uint32_t), stream_));
     for (DevArray<float4>* a : {&force_, &ppos_, &ppos_alt_, &phalf_, &pforce_})
         CK(cudaMemsetAsync(a->p, 0, cap * sizeof(float4), stream_));

@@ -95,6 +95,12 @@ void HostKernels::build(const lsp_params& p)
             }
     mass = p.rest_density / sum;
     if (p.mass_override > 0.f) mass = p.mass_override;
+    exact_tables = true;
+    for (int t : {1, 2, 4})
+        for (int i = 0; i <= sub; i++) {
+            const float a = std::fabs(tables[t * kTableSize + i]);
+            if (!(a == 0.f || (a >= 0x1p-29f && a <= 0x1p60f))) exact_tables = false;
+        }
 }
 
 float HostKernels::look(int t, float d) const
@@ -394,10 +400,12 @@ void Engine::ensure_grid()
     cells_ = cells;
     if (cells + 1 > cells_alloc_) {
         activate();
-        int64_t alloc = cells + 1;
+        // The scan reads and writes the histogram and cell table 8 entries at a time: both
+        // are padded to a multiple of 8 with zeros (scan_entries).
+        const int64_t alloc = scan_entries(cells + 1);
         hist_.alloc(alloc);
         cell_start_.alloc(alloc);
-        tile_sums_.alloc((alloc + 2047) / 2048 + 1);
+        tile_sums_.alloc(scan_tiles(cells + 1) + 1);
         CK(cudaMemsetAsync(hist_.p, 0, alloc * sizeof(uint32_t), stream_));
         CK(cudaMemsetAsync(cell_start_.p, 0, alloc * sizeof(uint32_t), stream_));
         cells_alloc_ = alloc;
@@ -461,6 +469,7 @@ DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt)
     P.keep_initial_velocity = p.keep_initial_velocity;
     P.min_it = p.pci_min_iterations;
     P.max_it = p.pci_max_iterations;
+    P.exact_tables = hk.exact_tables ? 1 : 0;
     return P;
 }
 

@@ -21,6 +21,10 @@ struct HostKernels {
     float h = 0, step = 0, mass = 0;
     float cut2 = 0;              // smallest float s with sqrt(s) >= h
     std::vector<float> tables;   // 5 x 1001 tables, then the slot thresholds on d and on d^2
+    // Every entry of the non-pressure pass's tables (poly6 gradient and Laplacian, viscosity
+    // Laplacian) is 0 or within [2^-29, 2^60]: the pass may then divide by the neighbour
+    // density with div_by (DevParams::exact_tables).
+    bool exact_tables = false;
     void build(const lsp_params& p);
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;

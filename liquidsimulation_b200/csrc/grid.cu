@@ -76,21 +76,36 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* w
     return warp_prefix + x - v;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, int64_t n,
+// The histogram and the cell table are padded with zeros to a multiple of 8 entries
+// (scan_entries): each thread moves its 8 consecutive entries as two 16-byte vectors. n8 is
+// the padded count.
+__device__ __forceinline__ void load8(const uint32_t* p, uint32_t (&v)[kScanItems])
+{
+    const uint4 a = *reinterpret_cast<const uint4*>(p);
+    const uint4 b = *reinterpret_cast<const uint4*>(p + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const uint32_t* __restrict__ in, int64_t n8,
                                                              uint32_t* __restrict__ tile_sums)
 {
     __shared__ uint32_t ws[32];
     const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
     uint32_t s = 0;
+    if (base < n8) {
+        uint32_t v[kScanItems];
+        load8(in + base, v);
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++)
-        if (base + j < n) s += in[base + j];
+        for (int j = 0; j < kScanItems; j++) s += v[j];
+    }
     uint32_t total;
     block_exclusive_scan(s, ws, &total);
     if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-// One block scans the tile sums in place (exclusive), chunk by chunk with a carry.
+// One block scans the tile sums in place (exclusive), chunk by chunk with a carry; only
+// launched when there are more than kFoldTiles tiles.
 __global__ void __launch_bounds__(1024) k_scan_top(uint32_t* tile_sums, int tiles)
 {
     __shared__ uint32_t ws[32];
@@ -106,29 +121,41 @@ __global__ void __launch_bounds__(1024) k_scan_top(uint32_t* tile_sums, int tile
     }
 }
 
-// Exclusive scan of the histogram into the dense cell table; clears the histogram for
-// the next step.
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restrict__ hist, int64_t n,
-                                                             const uint32_t* __restrict__ tile_sums,
+// Exclusive scan of the histogram into the dense cell table; clears the histogram for the
+// next step. With fold, the block sums the tile totals before its own tile (up to kFoldTiles
+// of them) itself; otherwise k_scan_top has turned tile_sums into those prefixes.
+constexpr int kFoldTiles = 4096;
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restrict__ hist, int64_t n8,
+                                                             const uint32_t* __restrict__ tile_sums, int fold,
                                                              uint32_t* __restrict__ out)
 {
     __shared__ uint32_t ws[32];
+    uint32_t prefix;
+    if (fold) {
+        uint32_t s = 0;
+        for (int k = threadIdx.x; k < (int)blockIdx.x; k += blockDim.x) s += tile_sums[k];
+        block_exclusive_scan(s, ws, &prefix);
+    } else {
+        prefix = tile_sums[blockIdx.x];
+    }
     const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanItems;
-    uint32_t v[kScanItems];
+    uint32_t v[kScanItems] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (base < n8) load8(hist + base, v);
     uint32_t s = 0;
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-        v[j] = base + j < n ? hist[base + j] : 0u;
-        s += v[j];
-    }
-    uint32_t ex = block_exclusive_scan(s, ws, nullptr) + tile_sums[blockIdx.x];
+    for (int j = 0; j < kScanItems; j++) s += v[j];
+    uint32_t ex = block_exclusive_scan(s, ws, nullptr) + prefix;
+    if (base < n8) {
+        uint32_t o[kScanItems];
 #pragma unroll
-    for (int j = 0; j < kScanItems; j++) {
-        if (base + j < n) {
-            out[base + j] = ex;
-            hist[base + j] = 0u;
+        for (int j = 0; j < kScanItems; j++) {
+            o[j] = ex;
+            ex += v[j];
         }
-        ex += v[j];
+        *reinterpret_cast<uint4*>(out + base) = make_uint4(o[0], o[1], o[2], o[3]);
+        *reinterpret_cast<uint4*>(out + base + 4) = make_uint4(o[4], o[5], o[6], o[7]);
+        *reinterpret_cast<uint4*>(hist + base) = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4*>(hist + base + 4) = make_uint4(0u, 0u, 0u, 0u);
     }
 }
 
@@ -166,8 +193,14 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
         atomicOr(&st->error_flags, kErrScan);
     }
     uint32_t dest = beg + rank;
-    opos[dest] = ipos[e.x];
-    ovel[dest] = ivel[e.x];
+    const float4 x = ipos[e.x], v = ivel[e.x];
+    opos[dest] = x;
+    ovel[dest] = v;
+    // The non-pressure pass divides pair terms by densities with div_by while every position
+    // and velocity of the step is in exact_div_safe's range.
+    if (!(exact_div_safe(x.x) && exact_div_safe(x.y) && exact_div_safe(x.z) && exact_div_safe(v.x) &&
+          exact_div_safe(v.y) && exact_div_safe(v.z)))
+        atomicOr(&st->np_unsafe, 1u);
     ohalf[dest] = ihalf[e.x];
     oold[dest] = iold[e.x];
     if (ohist) ohist[dest] = ihist[e.x];
@@ -202,6 +235,7 @@ __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
         if (pr < 0.f) pr *= P.neg;
         rho[i] = r;
         pres[i] = pr;
+        if (!exact_div_density(r)) atomicOr(&st->np_unsafe, 1u);
     }
     record_neighbor_count(P, c, valid, st);
 }
@@ -219,12 +253,13 @@ int launch_grid_keys(const GridBuildArgs& a, cudaStream_t s)
 
 int launch_grid_scan(const GridBuildArgs& a, cudaStream_t s)
 {
-    const int64_t n = (int64_t)a.P.cells + 1;
-    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
-    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
-    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
-    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
-    return 3;
+    const int64_t n8 = scan_entries((int64_t)a.P.cells + 1);
+    const int tiles = (int)scan_tiles((int64_t)a.P.cells + 1);
+    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n8, a.tile_sums);
+    const int fold = tiles <= kFoldTiles ? 1 : 0;
+    if (!fold) k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
+    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n8, a.tile_sums, fold, a.cell_start);
+    return fold ? 2 : 3;
 }
 
 int launch_grid_scatter(const GridBuildArgs& a, cudaStream_t s)
@@ -248,12 +283,7 @@ int launch_grid_order(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;
     const DevParams& P = a.P;
-    const int64_t n = (int64_t)P.cells + 1;
-    const int tiles = (int)((n + kScanTile - 1) / kScanTile);
-    k_scan_tiles<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums);
-    k_scan_top<<<1, 1024, 0, s>>>(a.tile_sums, tiles);
-    k_scan_apply<<<tiles, kScanThreads, 0, s>>>(a.hist, n, a.tile_sums, a.cell_start);
-    int launches = 3;
+    int launches = launch_grid_scan(a, s);
     if (P.n > 0) {
         k_scatter<<<blocks_for(P.n, T), T, 0, s>>>(P, a.pos_in, a.key, a.slot, a.cell_start, a.tmp);
         k_rank_gather<<<blocks_for(P.n, T), T, 0, s>>>(P, a.tmp, a.key, a.cell_start, a.pos_in, a.vel_in,

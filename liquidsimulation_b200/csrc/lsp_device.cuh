@@ -52,7 +52,9 @@ struct DevStatus {
     float last_ratio;
     int32_t last_k;             // logical index of the loop's last iteration (persistent loop)
     uint32_t div_unsafe;        // a predicted position left exact_div_safe's range this step
-    uint32_t pad[3];
+    uint32_t np_unsafe;         // a start-of-step position, velocity or density left the range
+                                // where the non-pressure pass divides with div_by
+    uint32_t pad[2];
 };
 
 struct DevParams {
@@ -90,6 +92,7 @@ struct DevParams {
     uint32_t cell_base;
     int coll_off;
     int scene;
+    int exact_tables;   // HostKernels::exact_tables
 };
 
 // ----------------------------------------------------------------- vector ops
@@ -127,7 +130,7 @@ __device__ __forceinline__ float4 f4(V3 a, float w) { return make_float4(a.x, a.
 // RN(a / d). recip_rn is checked against the IEEE reciprocal for every positive normal
 // float and div_by against IEEE division on billions of pairs
 // (tests/cpp/exact_div_check.cu). The theorem needs every value normal: callers use them
-// only where 2^-62 <= d <= 2^28 and a is 0 or 2^-62 <= |a| <= d (exact_div_safe). A zero
+// only where 2^-51 <= d <= 2^28 and a is 0 or 2^-51 <= |a| <= d (exact_div_safe). A zero
 // numerator gives a zero of either sign, which adds to a sum started at +0 like the IEEE
 // quotient's zero does.
 __device__ __forceinline__ float recip_rn(float d)
@@ -143,13 +146,32 @@ __device__ __forceinline__ float div_by(float a, float d, float y)
     const float r = __fmaf_rn(-d, q0, a);
     return __fmaf_rn(r, y, q0);
 }
-// A coordinate with which every pair difference and its quotient by the pair distance stay
-// where div_by is exact: 0, or 2^-39 <= |c| <= 2^26 (nonzero differences of such floats are
-// at least 2^-62 and distances at most 2^28).
+// The IEEE square root of s in the same style: the approximate reciprocal square root, then
+// one correction with the exact residual s - g^2 (Markstein's square-root step). Equal to
+// the IEEE square root for every float s >= 2^-102 (checked for every one on the GPU,
+// tests/cpp/exact_div_check.cu); below that the residual underflows and it is not exact.
+// s = 0 gives NaN where IEEE gives 0: the force pass only takes it for pairs j != i, whose
+// direction is 0 / 0 = NaN either way at zero distance.
+__device__ __forceinline__ float sqrt_rn(float s)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(s));
+    const float g = __fmul_rn(s, y);
+    const float h = __fmul_rn(0.5f, y);
+    const float r = __fmaf_rn(-g, g, s);
+    return __fmaf_rn(r, h, g);
+}
+// A density the non-pressure pass may divide by with div_by: 2^-20 <= rho <= 2^20 (so that
+// with numerators 0 or at least 2^-80 in magnitude every quotient and residual stays normal).
+__device__ __forceinline__ bool exact_div_density(float r) { return r >= 0x1p-20f && r <= 0x1p20f; }
+// A coordinate with which every pair difference, its squared length and its quotient by the
+// pair distance stay where sqrt_rn and div_by are exact: 0, or 2^-28 <= |c| <= 2^26 (nonzero
+// differences of such floats are at least 2^-51, squared lengths at least 2^-102 and at most
+// 3 * 2^54, distances at most 2^28).
 __device__ __forceinline__ bool exact_div_safe(float c)
 {
     const float a = fabsf(c);
-    return a == 0.f || (a >= 0x1p-39f && a <= 0x1p26f);
+    return a == 0.f || (a >= 0x1p-28f && a <= 0x1p26f);
 }
 
 // SPHKernel::get*Weight (SPHKernel.cpp:13-44): zero at or beyond h, else the table

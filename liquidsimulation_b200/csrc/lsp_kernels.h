@@ -75,6 +75,12 @@ struct StepBuffers {
     DevStatus* status;
 };
 
+// Entries of the histogram and cell-table buffers for `n` live entries: the scan moves them
+// 8 at a time, so both are padded to a multiple of 8 (the padding stays zero); and the scan's
+// tiles of 2048 entries.
+inline int64_t scan_entries(int64_t n) { return (n + 7) / 8 * 8; }
+inline int64_t scan_tiles(int64_t n) { return (scan_entries(n) + 2047) / 2048; }
+
 // All return the number of kernels launched.
 int launch_grid_sort(const GridBuildArgs& a, cudaStream_t s);
 // The part of the grid build after the keys: scan of a.hist (a.P.cells + 1 counters) into

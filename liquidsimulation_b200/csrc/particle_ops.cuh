@@ -183,9 +183,15 @@ __device__ __forceinline__ void density_one(const DevParams& P, const StepBuffer
 // three with the same per-sum rounding. kGrad adds |grad rho|, a warm-start feature. The
 // distance serves only the tables (the normal sums the unnormalised difference), so the
 // slot comes from the squared distance (slot records NA / NB on d^2).
-template <bool kGrad>
-__device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float4* NA,
-                                                const float4* NB, int i)
+//
+// With kExactDiv its seven quotients by the neighbour density per pair come from one
+// reciprocal of rho_j (recip_rn, div_by): the same bits while the step's positions,
+// velocities and densities are in range (DevStatus::np_unsafe clear) and the tables' entries
+// are (DevParams::exact_tables), since every numerator is then 0 or at least 2^-80 in
+// magnitude (nonpressure_one chooses).
+template <bool kGrad, bool kExactDiv>
+__device__ __forceinline__ void nonpressure_walk(const DevParams& P, const StepBuffers& b, const float4* NA,
+                                                 const float4* NB, int i)
 {
     const V3 xi = v3(b.pos[i]);
     const V3 vi = v3(b.vel[i]);
@@ -208,10 +214,23 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
                              // |x_i - x_j|^2 equals |x_j - x_i|^2 bit for bit
                              const NonpressureWeights at(NA, NB, sqmag(dir), P);
                              const float w_dw = at.dw;
-                             normal += dir * w_dw / r.rho;
-                             lap += at.d2w / r.rho;
-                             if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at.vd2w;
-                             if (kGrad) grad += dir * (w_dw * ((r.rho - rhoi) / r.rho));
+                             if (kExactDiv) {
+                                 const float y = recip_rn(r.rho);
+                                 auto q = [&](float a) { return div_by(a, r.rho, y); };
+                                 const V3 n = dir * w_dw;
+                                 normal += v3(q(n.x), q(n.y), q(n.z));
+                                 lap += q(at.d2w);
+                                 if (j != i) {
+                                     const V3 dv = v3(r.v) - vi;
+                                     visc += v3(q(dv.x), q(dv.y), q(dv.z)) * at.vd2w;
+                                 }
+                                 if (kGrad) grad += dir * (w_dw * q(r.rho - rhoi));
+                             } else {
+                                 normal += dir * w_dw / r.rho;
+                                 lap += at.d2w / r.rho;
+                                 if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at.vd2w;
+                                 if (kGrad) grad += dir * (w_dw * ((r.rho - rhoi) / r.rho));
+                             }
                          });
     if (kGrad) b.gradrho[i] = P.mass * mag(grad);
     normal *= P.mass;
@@ -220,6 +239,15 @@ __device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBu
     visc *= P.viscosity * P.mass;
     F += visc;
     b.force[i] = f4(F, 0.f);
+}
+template <bool kGrad>
+__device__ __forceinline__ void nonpressure_one(const DevParams& P, const StepBuffers& b, const float4* NA,
+                                                const float4* NB, int i)
+{
+    if (P.exact_tables && *(const volatile uint32_t*)&b.status->np_unsafe == 0u)
+        nonpressure_walk<kGrad, true>(P, b, NA, NB, i);
+    else
+        nonpressure_walk<kGrad, false>(P, b, NA, NB, i);
 }
 
 // SPHSolver::accumulatePressureForces, CPU branch (SPHSolver.cpp:268-290).
@@ -342,9 +370,10 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 
 // PCISPHSolver.cpp:129-150 for one particle. s = p / rho*^2 is the per-particle factor the
 // reference recomputes per pair; the prefactor uses the current density rho_i. The pair
-// direction (x_i - x_j) / d is three IEEE quotients; with kExactDiv they come from one
-// reciprocal of d (recip_rn, div_by), the same bits for the predicted positions the step's
-// predict passes found safe (DevStatus::div_unsafe clear).
+// distance is an IEEE square root and the direction (x_i - x_j) / d three IEEE quotients;
+// with kExactDiv they come from sqrt_rn and one reciprocal of d (recip_rn, div_by), the same
+// bits for the predicted positions the step's predict passes found safe
+// (DevStatus::div_unsafe clear).
 template <bool kExactDiv>
 __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuffers& b, const float* SDW,
                                                const float* TH, int i, const float4* ppos)
@@ -360,7 +389,7 @@ __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuf
                              // |x_i - x_j| rounds exactly like the reference's |x_j - x_i|
                              // (the squares are equal), so one difference serves both.
                              const V3 dq = xi - v3(pj4);
-                             const float d = mag(dq);
+                             const float d = kExactDiv ? sqrt_rn(sqmag(dq)) : mag(dq);
                              V3 dir;
                              if (kExactDiv) {
                                  const float y = recip_rn(d);

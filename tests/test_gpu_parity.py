@@ -94,6 +94,28 @@ def test_grid_build_matches_spec(oracle_mod):
     gpu.close()
 
 
+def test_grid_build_with_many_scan_tiles(oracle_mod):
+    """A grid box of 225^3 = 11.4M cells (5,563 scan tiles of 2,048 cells, more than the 4,096
+    whose prefixes the apply kernel sums itself): the tile prefixes come from the separate
+    top-level scan. Same keys, order and cell table as the specification, and the step
+    matches the oracle."""
+    sc = scenes.small_box_scene(n_side=(10, 12, 10))
+    sc.domain = ((0.0, 0.0, 0.0), (9.0, 9.0, 9.0))
+    gpu = from_scene(sc)
+    orc = oracle_mod.OracleSolver(sc)
+    gpu.update(sc.dt)
+    orc.step(sc.dt)
+    dims, org, keys, ids, start = gpu.grid()
+    assert int(np.prod(dims.astype(np.int64))) > 4096 * 2048
+    k2, i2, s2, esc = oracle_mod.grid_build(sc.positions, gpu.get_kernel_radius(), org, dims)
+    assert esc == 0
+    assert np.array_equal(keys, k2) and np.array_equal(ids, i2) and np.array_equal(start, s2)
+    for f in (abi.FIELD_POSITION, abi.FIELD_DENSITY, abi.FIELD_PRESSURE):
+        assert bits_equal(gpu.read(f), orc.get(f)), f
+    gpu.close()
+    orc.close()
+
+
 @pytest.mark.parametrize("solver", [abi.LSP_SOLVER_SPH, abi.LSP_SOLVER_PCISPH])
 def test_small_scene_bit_exact(oracle_mod, solver):
     sc = scenes.small_box_scene(solver=solver)
