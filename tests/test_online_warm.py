@@ -116,3 +116,22 @@ def test_online_warm_start_on_a_solver():
     assert pol.trained_steps == pol.training_steps == 6 and sum(tried) == 10
     a.close()
     plain.close()
+
+
+@pytest.mark.gpu
+def test_set_warm_start_switches_mode_only():
+    """lsp_set_warm_start changes params.warm_start and nothing else; an unknown mode is
+    refused with LSP_ERR_INVALID and leaves the solver as it was."""
+    from liquidsimulation_b200.solver import from_scene
+    sc = scenes.dam_break_pcisph(seed=5, counts=(8, 10, 8), s=0.02)
+    s = from_scene(sc)
+    before = s.params
+    s.set_warm_start(abi.LSP_WARM_MLP)
+    after = s.params
+    assert after.warm_start == abi.LSP_WARM_MLP
+    after.warm_start = before.warm_start
+    assert bytes(after) == bytes(before)
+    with pytest.raises(abi.LspError) as e:
+        s.set_warm_start(7)
+    assert e.value.code == abi.LSP_ERR_INVALID and s.params.warm_start == abi.LSP_WARM_MLP
+    s.close()
