@@ -21,6 +21,7 @@ namespace lsp {
 // reference, and rounded to float.
 void HostKernels::build(const lsp_params& p)
 {
+    denom_ready_ = false;
     const int sub = kTableSize - 1;
     h = p.kernel_radius_factor * p.particle_radius;
     float r2 = h * h, r3 = r2 * h, r4 = r3 * h, r5 = r4 * h, r6 = r5 * h, r9 = r6 * r3;
@@ -110,8 +111,25 @@ float HostKernels::look(int t, float d) const
     return tables[t * kTableSize + key];
 }
 
-// PCISPHSolver::calcDelta (PCISPHSolver.cpp:286-328).
+// PCISPHSolver::calcDelta (PCISPHSolver.cpp:286-328). The lattice sum depends on the
+// parameters only, so it is kept for the particle radius it was summed for (the engine asks
+// for delta every step); beta and delta follow per time step, in the reference's order.
 float HostKernels::delta(const lsp_params& p, float dt) const
+{
+    if (!(denom_ready_ && denom_radius_ == p.particle_radius)) {
+        denom_ = lattice_denominator(p);
+        denom_radius_ = p.particle_radius;
+        denom_ready_ = true;
+    }
+    const float denom = denom_;
+    float beta = dt * mass / p.rest_density;
+    beta = 2.f * beta * beta;
+    float delta = 0.f;
+    if (std::fabs(denom) > 0.f) delta = -1.f / (beta * denom);
+    return delta;
+}
+
+float HostKernels::lattice_denominator(const lsp_params& p) const
 {
     float stepSize = 1.6f * p.particle_radius;
     float d1x = 0.f, d1y = 0.f, d1z = 0.f, d2 = 0.f;
@@ -128,12 +146,7 @@ float HostKernels::delta(const lsp_params& p, float dt) const
                     d2 += gx * gx + gy * gy + gz * gz;
                 }
             }
-    float denom = -(d1x * d1x + d1y * d1y + d1z * d1z) - d2;
-    float beta = dt * mass / p.rest_density;
-    beta = 2.f * beta * beta;
-    float delta = 0.f;
-    if (std::fabs(denom) > 0.f) delta = -1.f / (beta * denom);
-    return delta;
+    return -(d1x * d1x + d1y * d1y + d1z * d1z) - d2;
 }
 
 // ------------------------------------------------------------------ engine

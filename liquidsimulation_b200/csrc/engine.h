@@ -28,6 +28,12 @@ struct HostKernels {
     void build(const lsp_params& p);
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;
+
+private:
+    float lattice_denominator(const lsp_params& p) const;
+    // calcDelta's lattice sum, computed on the first delta() after build() (build resets it).
+    mutable float denom_ = 0.f, denom_radius_ = 0.f;
+    mutable bool denom_ready_ = false;
 };
 
 // Parameter checks shared by single scenes and batches (LSP_ERR_INVALID on failure).
