@@ -78,3 +78,18 @@ def test_library_arm_line():
     assert d["config"] == _our_config(["--steps", "3", "--warmup", "3", "--train-steps", "5", "--long-steps", "0"])
     ss = d["same_state"]
     assert len(ss) == 2 and all(x["samples"] > 0 for x in ss)
+    for x in ss:
+        assert x["device_time_ratio"] > 0
+        if x["plain"]["qualifying"] == 0:
+            assert x["learned_vs_plain_same_state"] is None and not x["target_met"]
+
+
+def test_same_state_ratio_counts_only_qualifying_steps():
+    """learned_vs_plain_same_state is the metric's ratio (steps that met eta per device time),
+    so a run where the plain steps never met eta has no ratio, however the times compare."""
+    import bench
+    assert bench.qualifying_ratio(20, 40.0, 20, 44.0) == pytest.approx(40.0 / 44.0)
+    assert bench.qualifying_ratio(10, 40.0, 20, 40.0) == pytest.approx(2.0)
+    assert bench.qualifying_ratio(0, 460.0, 0, 250.0) is None
+    assert bench.qualifying_ratio(0, 460.0, 5, 250.0) is None
+    assert bench.qualifying_ratio(20, 40.0, 0, 44.0) == 0.0

@@ -94,6 +94,66 @@ def test_grid_build_matches_spec(oracle_mod):
     gpu.close()
 
 
+def _edge_scene(O, solver):
+    """Particles at the edges of the neighbour search (SPHSpatialGrid.cpp:39-82): a block
+    straddling the origin (negative cells, and cell 0, which spans (-h, h) under the
+    truncating cell coordinate), particles exactly on cell faces and one ulp either side, and
+    pairs whose distance lies within a few ulp of h in random directions. (Particles clamped
+    into the border cells of a user grid box are covered by test_particles_outside_grid_box.)"""
+    s = 0.02
+    params = scenes._params(s, solver, pci_min_iterations=1, pci_max_iterations=4)
+    block = scenes.lattice((-0.1, -0.08, -0.06), (10, 8, 7), s, 11)
+    probe = O.OracleSolver(scenes.Scene("probe", params, block, np.zeros_like(block), [], 0.0005, 1))
+    h = np.float32(probe.kernel_radius())
+    probe.close()
+    rng = np.random.default_rng(12)
+    pts = [block]
+    for k in range(-3, 4):
+        f = np.float32(k) * h
+        for v in (np.nextafter(f, np.float32(-1)), f, np.nextafter(f, np.float32(1))):
+            p = rng.uniform(-0.09, 0.09, (3, 3)).astype(np.float32)
+            for a in range(3):
+                p[a, a] = v
+            pts.append(p)
+    base = rng.uniform(-0.09, 0.09, (120, 3)).astype(np.float32)
+    d = rng.normal(size=(120, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.float64(h) * (1.0 + rng.integers(-3, 4, (120, 1)) * 2.0 ** -23)
+    pts += [base, (base + d * r).astype(np.float32)]
+    pos = np.concatenate(pts).astype(np.float32)
+    cols = [scenes.Collider("box", (0.0, 0.0, 0.0), (0.3, 0.3, 0.3), True)]
+    return scenes.Scene("search_edges", params, pos, np.zeros_like(pos), cols, 0.0005, 2, spacing=s), h
+
+
+@pytest.mark.parametrize("solver", [abi.LSP_SOLVER_SPH, abi.LSP_SOLVER_PCISPH])
+def test_neighbour_search_edges(oracle_mod, solver):
+    sc, h = _edge_scene(oracle_mod, solver)
+    gpu, orc = from_scene(sc), oracle_mod.OracleSolver(sc)
+    fields = FIELDS_PCI if solver == abi.LSP_SOLVER_PCISPH else FIELDS_SPH
+    try:
+        for step in range(3):
+            sg, so = gpu.update(sc.dt), orc.step(sc.dt)
+            assert sg.iterations == so.iterations, step
+            og, ig = gpu.neighbors()
+            oo, io = orc.neighbors()
+            assert np.array_equal(og, oo) and np.array_equal(ig, io), f"step {step}: neighbour lists differ"
+            for f in fields:
+                a, b = gpu.read(f), orc.get(f)
+                assert bits_equal(a, b), f"step {step} field {f}: {mismatch_report(a, b)}"
+            if step == 0:
+                # The scene does reach the edges: accepted pairs of the first step's lists
+                # whose squared distance lies within 2^-20 of h^2, and particles in cell 0
+                # from both sides of the origin.
+                assert (np.abs(sc.positions) < h).all(axis=1).sum() > 0
+                assert (sc.positions < -h).all(axis=1).sum() > 0
+                owner = np.repeat(np.arange(sc.n), np.diff(og))
+                d2 = ((sc.positions[ig].astype(np.float64) - sc.positions[owner]) ** 2).sum(axis=1)
+                assert (np.abs(d2 / np.float64(h) ** 2 - 1.0) < 2.0 ** -20).sum() > 0
+    finally:
+        gpu.close()
+        orc.close()
+
+
 def test_grid_build_with_many_scan_tiles(oracle_mod):
     """A grid box of 225^3 = 11.4M cells (5,563 scan tiles of 2,048 cells, more than the 4,096
     whose prefixes the apply kernel sums itself): the tile prefixes come from the separate
