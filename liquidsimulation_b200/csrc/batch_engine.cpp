@@ -205,7 +205,6 @@ void BatchEngine::build()
 
     CK(cudaMemsetAsync(hist_.p, 0, scan_entries(cells_ + 1) * sizeof(uint32_t), stream_));
     CK(cudaMemsetAsync(cell_start_.p, 0, scan_entries(cells_ + 1) * sizeof(uint32_t), stream_));
-    CK(cudaMemsetAsync(cell_start_.p, 0, (cells_ + 1) * sizeof(uint32_t), stream_));
     for (DevArray<float4>* a : {&force_, &ppos_, &ppos_alt_, &phalf_, &pforce_})
         CK(cudaMemsetAsync(a->p, 0, cap * sizeof(float4), stream_));
     for (DevArray<float>* a : {&rho_, &pres_, &prho_, &err_}) CK(cudaMemsetAsync(a->p, 0, cap * sizeof(float), stream_));
