@@ -168,7 +168,9 @@ int lsp_set_domain(lsp_solver* s, const float lo[3], const float hi[3]);
 /* ---- stepping ---- */
 /* PhysicSolver::update(dt) (PhysicSolver.cpp:12-21): one full step. */
 int lsp_step(lsp_solver* s, float dt, lsp_step_stats* stats);
-/* n steps back to back without host synchronisation in between (stats of the last). */
+/* n steps in one call, stats of the last. Each step still reads its status word back before
+ * the next is queued (a step whose neighbour lists overflow is redone with larger lists), so
+ * this saves the per-call overhead, not the per-step synchronisation. */
 int lsp_step_many(lsp_solver* s, float dt, int steps, lsp_step_stats* stats);
 int lsp_synchronize(lsp_solver* s);
 

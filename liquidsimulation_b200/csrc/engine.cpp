@@ -733,9 +733,8 @@ int grown_neighbor_capacity(int needed, int current)
     return (int)std::max<int64_t>(needed, std::min<int64_t>(c, 4096));
 }
 
-void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
+void Engine::run_step(float dt, lsp_step_stats* st)
 {
-    (void)final_sync;
     if (st) std::memset(st, 0, sizeof(*st));
     if (!(dt > 0.f) || !std::isfinite(dt)) throw Error(LSP_ERR_INVALID, "dt must be finite and > 0");
     if (n_ == 0) {
@@ -832,12 +831,12 @@ void Engine::run_step(float dt, lsp_step_stats* st, bool final_sync)
         throw Error(LSP_ERR_NOT_CONVERGED, "PCISPH reached max iterations above eta");
 }
 
-void Engine::step(float dt, lsp_step_stats* st) { run_step(dt, st, true); }
+void Engine::step(float dt, lsp_step_stats* st) { run_step(dt, st); }
 
 void Engine::step_many(float dt, int steps, lsp_step_stats* st)
 {
     if (steps < 0) throw Error(LSP_ERR_INVALID, "steps must be >= 0");
-    for (int s = 0; s < steps; s++) run_step(dt, st, s == steps - 1);
+    for (int s = 0; s < steps; s++) run_step(dt, st);
 }
 
 void Engine::synchronize()

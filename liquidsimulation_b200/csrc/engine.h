@@ -135,7 +135,7 @@ private:
     void ensure_grid();
     void ensure_neighbors(int cap);
     void upload_colliders();
-    void run_step(float dt, lsp_step_stats* st, bool final_sync);
+    void run_step(float dt, lsp_step_stats* st);
     // Returns true when the persistent device loop ran (its stats arrive with the status).
     bool pcisph_loop(const DevParams& P, const StepBuffers& b, lsp_step_stats* st);
     void stage(size_t floats);
