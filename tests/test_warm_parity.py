@@ -7,8 +7,8 @@ its own correction (:117-125). The loop then runs as the reference's (:64-163); 
 iteration 1 the guess is rejected, and the step restarts from the zero start, if the
 maximum density error rose. The oracle restates exactly that (OracleSolver.step with
 initial_pressure), so a step whose guess was KEPT is compared with the oracle started from
-the same guess: every field to 0 ulp, the same iteration count and the same verdict on
-the guess. The guess itself is recomputed here from the step's recorded features with
+the same guess: every field to 0 ulp, the same iteration count and the same decision to
+keep or reject the guess. The guess itself is recomputed here from the step's recorded features with
 lsp_mlp_forward, which runs the same tensor-core tile as the warm-start kernel.
 """
 import numpy as np
