@@ -343,42 +343,50 @@ __device__ __forceinline__ void collide_all(const Collider* cols, int ncoll, V3&
     for (int c = 0; c < ncoll; c++) collide(cols[c], pos, vel, P);
 }
 
-// Walks particle i's neighbour list (column-major, `stride` apart) in list order, software
-// pipelined: while batch b's records are fetched and its pairs computed, the indices of
-// batch b+1 are already in flight, so the list's DRAM latency overlaps the arithmetic.
-// f(j, record) runs strictly in list order, so every sum accumulates in the reference's
-// order.
+// Neighbour-list layout: entry k of particle i is component k & 3 of the int4 at group k >> 2,
+// and each group is column-major over the particles (group g of particle i at
+// ((int4*)nbr)[g * stride + i]). A reader fetches four indices with one coalesced 16-byte
+// load; the builder writes four entries with one store instead of four scattered 4-byte
+// ones (each a separate L2 request: the list build is bound by their rate).
+__device__ __forceinline__ int list_entry(const int32_t* __restrict__ nbr, int64_t stride, int64_t i, int k)
+{
+    return nbr[(((int64_t)(k >> 2) * stride + i) << 2) + (k & 3)];
+}
+
+// Walks particle i's neighbour list in list order, software pipelined: while a group's
+// records are fetched and its pairs computed (B records at a time, B = 1, 2 or 4), the next
+// group's four indices are already in flight, so the list's DRAM latency overlaps the
+// arithmetic. f(j, record) runs strictly in list order, so every sum accumulates in the
+// reference's order.
 template <int B, typename Load, typename F>
-__device__ __forceinline__ void for_each_neighbor(const int32_t* __restrict__ list, int64_t stride, int cnt,
+__device__ __forceinline__ void for_each_neighbor(const int32_t* __restrict__ nbr, int i, int64_t stride, int cnt,
                                                   Load load, F f)
 {
-    const int full = cnt / B;
-    int j[B];
-    if (full > 0) {
+    static_assert(B == 1 || B == 2 || B == 4, "a walk batch divides the 4-entry group");
+    const int4* g = reinterpret_cast<const int4*>(nbr) + i;
+    const int full = cnt >> 2;
+    const int rest = cnt & 3;
+    int4 cur = make_int4(0, 0, 0, 0);
+    if (cnt > 0) cur = __ldg(g);
+    for (int q = 0; q < full; q++) {
+        g += stride;
+        int4 nxt = make_int4(0, 0, 0, 0);
+        if (q + 1 < full || rest) nxt = __ldg(g);
+        const int j[4] = {cur.x, cur.y, cur.z, cur.w};
 #pragma unroll
-        for (int u = 0; u < B; u++) j[u] = __ldg(list + u * stride);
-        list += B * stride;
-    }
-    for (int b = 0; b < full; b++) {
-        decltype(load(0)) r[B];
+        for (int s0 = 0; s0 < 4; s0 += B) {
+            decltype(load(0)) r[B];
 #pragma unroll
-        for (int u = 0; u < B; u++) r[u] = load(j[u]);
-        int jn[B];
-        if (b + 1 < full) {
+            for (int u = 0; u < B; u++) r[u] = load(j[s0 + u]);
 #pragma unroll
-            for (int u = 0; u < B; u++) jn[u] = __ldg(list + u * stride);
-            list += B * stride;
+            for (int u = 0; u < B; u++) f(j[s0 + u], r[u]);
         }
-#pragma unroll
-        for (int u = 0; u < B; u++) f(j[u], r[u]);
-#pragma unroll
-        for (int u = 0; u < B; u++) j[u] = jn[u];
+        cur = nxt;
     }
-    for (int e = full * B; e < cnt; e++) {
-        int jj = __ldg(list);
-        list += stride;
-        f(jj, load(jj));
-    }
+    // The last, partial group: its first `rest` components.
+    if (rest > 0) f(cur.x, load(cur.x));
+    if (rest > 1) f(cur.y, load(cur.y));
+    if (rest > 2) f(cur.z, load(cur.z));
 }
 
 // Cell coordinate of the reference's CPU grid (SPHSpatialGrid.cpp:80-82).

@@ -82,9 +82,12 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
         lo[a] = min(max(lo[a], o[a]), o[a] + d[a] - 1) - o[a];
         hi[a] = min(max(hi[a], o[a]), o[a] + d[a] - 1) - o[a];
     }
-    const int cap = P.nbr_cap;
+    const int cap = P.nbr_cap;   // a multiple of 4: whole groups
     const int64_t stride = P.nbr_stride;
-    int32_t* out = nbr + i;
+    // Accepted entries shift through `grp` (the newest in .w) and go out four at a time
+    // (list_entry's layout).
+    int4* out = reinterpret_cast<int4*>(nbr) + i;
+    int4 grp = make_int4(0, 0, 0, 0);
     int c = 0;
     if (lo[2] <= hi[2]) {
         for (int cx = lo[0]; cx <= hi[0]; cx++) {
@@ -100,8 +103,11 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
                     if (s <= P.h2) {
                         if (kDensity) sum += lookup_sq(W, TH2, s, P);
                         if (c < cap) {
-                            *out = q;
-                            out += stride;
+                            grp = make_int4(grp.y, grp.z, grp.w, q);
+                            if ((c & 3) == 3) {
+                                *out = grp;
+                                out += stride;
+                            }
                         }
                         c++;
                     }
@@ -109,6 +115,12 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
             }
         }
     }
+    // The last, partial group: its `rest` entries sit in the top components (its unused
+    // components are never read).
+    const int rest = c < cap ? (c & 3) : 0;
+    if (rest == 1) *out = make_int4(grp.w, 0, 0, 0);
+    if (rest == 2) *out = make_int4(grp.z, grp.w, 0, 0);
+    if (rest == 3) *out = make_int4(grp.y, grp.z, grp.w, 0);
     if (kDensity) *wsum = sum;
     return c;
 }
@@ -167,7 +179,7 @@ __device__ __forceinline__ void density_one(const DevParams& P, const StepBuffer
 {
     const V3 xi = v3(b.pos[i]);
     float sum = 0.f;
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<4>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return b.pos[j]; },
                          [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
     float rho = P.mass * sum;
@@ -206,7 +218,7 @@ __device__ __forceinline__ void nonpressure_walk(const DevParams& P, const StepB
         float4 x, v;
         float rho;
     };
-    for_each_neighbor<2>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<2>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return Rec{b.pos[j], b.vel[j], b.rho[j]}; },
                          [&](int j, const Rec& r) {
                              const V3 xj = v3(r.x);
@@ -262,7 +274,7 @@ __device__ __forceinline__ void sph_pressure_one(const DevParams& P, const StepB
         float4 x;
         float rho, p;
     };
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<4>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return Rec{b.pos[j], b.rho[j], b.pres[j]}; },
                          [&](int j, const Rec& r) {
                              if (j == i) return;
@@ -346,7 +358,7 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 {
     const V3 xi = v3(ppos[i]);
     float sum = 0.f;
-    for_each_neighbor<3>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<4>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return ppos[j]; },
                          [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
     float pd = P.mass * sum;
@@ -382,7 +394,7 @@ __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuf
     const V3 xi = v3(pi4);
     const float tf = pi4.w;
     V3 pf = v3(0.f, 0.f, 0.f);
-    for_each_neighbor<4>(b.nbr + i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor<2>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return ppos[j]; },
                          [&](int j, float4 pj4) {
                              if (j == i) return;

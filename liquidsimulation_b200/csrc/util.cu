@@ -143,7 +143,7 @@ __global__ void k_neighbor_export(const int32_t* __restrict__ nbr, const int32_t
     int32_t s = slot_of_id[id];
     int c = count[s];
     int64_t o = offsets[id];
-    for (int e = 0; e < c; e++) out[o + e] = id_of(pos[nbr[(int64_t)e * stride + s]]);
+    for (int e = 0; e < c; e++) out[o + e] = id_of(pos[list_entry(nbr, stride, s, e)]);
 }
 
 void launch_neighbor_export(const int32_t* nbr, const int32_t* count, int64_t stride, const float4* pos,

@@ -60,7 +60,7 @@ __device__ __forceinline__ float density_first(const DevParams& P, const StepBuf
         const V3 xi = v3(b.ppos[i]);
         const int cnt = __ldg(b.nbr_count + i);
         float sum = 0.f;
-        for_each_neighbor<4>(b.nbr + i, P.nbr_stride, cnt, [&](int j) { return b.ppos[j]; },
+        for_each_neighbor<4>(b.nbr, i, P.nbr_stride, cnt, [&](int j) { return b.ppos[j]; },
                              [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
         pd = P.mass * sum;
         float er = pd - P.rho0;
