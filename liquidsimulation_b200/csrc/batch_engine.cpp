@@ -250,6 +250,7 @@ void BatchEngine::ensure_neighbors(int cap)
     if (cap > 4096) throw Error(LSP_ERR_CAPACITY, "neighbour count above 4096 per particle");
     activate();
     nbr_.alloc((size_t)cap * (size_t)nbr_stride_);
+    nbr_src_.alloc((size_t)cap * (size_t)nbr_stride_);
     nbr_cap_ = cap;
     params_dirty_ = true;
     drop_graphs();
@@ -349,7 +350,7 @@ StepBuffers BatchEngine::buffers(int c)
     b.pos = pos_[c].p; b.vel = vel_[c].p; b.half = half_[c].p; b.old = old_[c].p;
     b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
-    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
+    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p + sc_.size();
     b.hist = history_on() ? phist_[c].p : nullptr;
     b.gradrho = features_on() ? gradrho_.p : nullptr;
@@ -380,7 +381,7 @@ int BatchEngine::enqueue_step(int c, int grid)
     g.status = status_.p + S;
     launches += launch_grid_order(g, stream_);
     StepBuffers b = buffers(1 - c);
-    launches += launch_batch_neighbors_density(a, pos_[1 - c].p, cell_start_.p, nbr_.p, nbr_count_.p, rho_.p,
+    launches += launch_batch_neighbors_density(a, pos_[1 - c].p, cell_start_.p, nbr_src_.p, nbr_count_.p, rho_.p,
                                                pres_.p, stream_);
     launches += launch_batch_nonpressure(a, b, stream_);
     if (pcisph_) {

@@ -117,7 +117,7 @@ private:
     DevArray<float> rho_, pres_, prho_, err_;
     DevArray<uint32_t> key_, slot_, sorted_key_, hist_, cell_start_, tile_sums_, loop_sync_, maxerr_;
     DevArray<int2> tmp_;
-    DevArray<int32_t> slot_of_id_, nbr_, nbr_count_;
+    DevArray<int32_t> slot_of_id_, nbr_, nbr_src_, nbr_count_;   // nbr_: grouped lists; nbr_src_: the build's plain lists
     DevArray<float> tables_, stage_;
     DevArray<Collider> dcols_;
     DevArray<DevParams> dparams_;

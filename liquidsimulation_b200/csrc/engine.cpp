@@ -289,6 +289,7 @@ void Engine::ensure_neighbors(int cap)
     if (cap > 4096) throw Error(LSP_ERR_CAPACITY, "neighbour count above 4096 per particle");
     nbr_stride_ = std::max<int64_t>(cap_, 256);
     nbr_.alloc((size_t)cap * (size_t)nbr_stride_);
+    nbr_src_.alloc((size_t)cap * (size_t)nbr_stride_);
     nbr_cap_ = cap;
 }
 
@@ -505,7 +506,7 @@ StepBuffers Engine::buffers()
     b.pos = pos_[cur_].p; b.vel = vel_[cur_].p; b.half = half_[cur_].p; b.old = old_[cur_].p;
     b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
-    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p;
+    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p;
     b.hist = phist_[cur_].p;
     b.gradrho = features_on() ? gradrho_.p : nullptr;
@@ -767,7 +768,7 @@ void Engine::run_step(float dt, lsp_step_stats* st)
         g.key = key_.p; g.slot = slot_.p; g.hist = hist_.p; g.tile_sums = tile_sums_.p; g.cell_start = cell_start_.p;
         g.tmp = tmp_.p; g.slot_of_id = slot_of_id_.p; g.sorted_key = sorted_key_.p;
         g.hist_in = phist_[cur_].p; g.hist_out = phist_[1 - cur_].p;
-        g.nbr = nbr_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
+        g.nbr = nbr_src_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
         // The neighbour build also sums the start-of-step density (k_neighbors_density).
         g.tables = tables_.p; g.rho = rho_.p; g.pres = pres_.p;
         timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_keys(g, stream_); });

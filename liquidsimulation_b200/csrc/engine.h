@@ -154,7 +154,7 @@ private:
     DevArray<float> rho_, pres_, prho_, err_;
     DevArray<uint32_t> key_, slot_, sorted_key_;
     DevArray<int2> tmp_;
-    DevArray<int32_t> slot_of_id_, nbr_, nbr_count_;
+    DevArray<int32_t> slot_of_id_, nbr_, nbr_src_, nbr_count_;   // nbr_: grouped lists; nbr_src_: the build's plain lists
     int nbr_cap_ = 0;
     int64_t nbr_stride_ = 0;
 

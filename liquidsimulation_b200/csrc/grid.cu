@@ -18,9 +18,9 @@
 //   k_scatter     particle -> (cell start + slot)
 //   k_rank_gather deterministic rank by caller id inside each cell, then one gather of
 //                 the 64-byte persistent state into the new order
-//   k_neighbors_density  the start-of-step neighbour lists (list_entry's grouped layout),
-//                 reference order, with the density and pressure summed over the accepted
-//                 pairs
+//   k_neighbors_density  the start-of-step neighbour lists (plain column-major; the
+//                 non-pressure pass regroups them), reference order, with the density and
+//                 pressure summed over the accepted pairs
 #include "lsp_kernels.h"
 #include "particle_ops.cuh"
 
@@ -209,13 +209,13 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
     sorted_key[dest] = k;
 }
 
-// Start-of-step neighbour lists (neighbors_one, list_entry's layout) plus the start-of-step density
+// Start-of-step neighbour lists (neighbors_one, plain column-major) plus the start-of-step density
 // and pressure of density_one (SPHSolver::calcParticleDensityPressure,
 // SPHSolver.cpp:442-463), summed while the list is built: a pass over the stored list and
 // its position gathers would cost more. (A list that
 // overflows its capacity raises the overflow flag and the step is redone, so the sum over
 // every accepted pair never differs from the stored list's.)
-__global__ void __launch_bounds__(256, 8) k_neighbors_density(DevParams P, const float4* __restrict__ pos,
+__global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
                                     const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
                                     int32_t* __restrict__ count, DevStatus* st, const float* __restrict__ tables,
                                     float* __restrict__ rho, float* __restrict__ pres)

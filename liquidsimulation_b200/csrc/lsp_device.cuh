@@ -353,6 +353,47 @@ __device__ __forceinline__ int list_entry(const int32_t* __restrict__ nbr, int64
     return nbr[(((int64_t)(k >> 2) * stride + i) << 2) + (k & 3)];
 }
 
+// for_each_neighbor (B = 2) over particle i's plain column-major list `src` (entry k at
+// src[k * stride + i]) that also stores the list in list_entry's grouped layout at `dst`: each
+// pair of entries goes out as one 8-byte store (half a group; all lanes store in step, so the
+// stores coalesce), and the next pair's indices are in flight while the current pair's records
+// are fetched and its pairs computed, as in for_each_neighbor.
+template <typename Load, typename F>
+__device__ __forceinline__ void for_each_neighbor_regroup(const int32_t* __restrict__ src, int32_t* __restrict__ dst,
+                                                          int i, int64_t stride, int cnt, Load load, F f)
+{
+    const int32_t* l = src + i;
+    int32_t* g = dst + 4 * (int64_t)i;   // the current group of particle i
+    const int full = cnt >> 1;
+    int j0 = 0, j1 = 0;
+    if (full > 0) {
+        j0 = __ldg(l);
+        j1 = __ldg(l + stride);
+        l += 2 * stride;
+    }
+    for (int b = 0; b < full; b++) {
+        const auto r0 = load(j0);
+        const auto r1 = load(j1);
+        int n0 = 0, n1 = 0;
+        if (b + 1 < full) {
+            n0 = __ldg(l);
+            n1 = __ldg(l + stride);
+            l += 2 * stride;
+        }
+        reinterpret_cast<int2*>(g)[b & 1] = make_int2(j0, j1);
+        if (b & 1) g += 4 * stride;
+        f(j0, r0);
+        f(j1, r1);
+        j0 = n0;
+        j1 = n1;
+    }
+    if (cnt & 1) {
+        const int jj = __ldg(l);
+        g[2 * (full & 1)] = jj;
+        f(jj, load(jj));
+    }
+}
+
 // Walks particle i's neighbour list in list order, software pipelined: while a group's
 // records are fetched and its pairs computed (B records at a time, B = 1, 2 or 4), the next
 // group's four indices are already in flight, so the list's DRAM latency overlaps the

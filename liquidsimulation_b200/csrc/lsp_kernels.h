@@ -66,9 +66,15 @@ struct StepBuffers {
     float* err;
     float4* hist;             // warm-start pressure history, null when off
     float* gradrho;           // |grad rho|, null when off
-    // neighbours
+    // neighbours: the lists in list_entry's grouped layout (nbr), read by every walk after
+    // the non-pressure pass. The neighbour build writes them plain column-major (nbr_src,
+    // entry k of particle i at nbr_src[k * stride + i]: one 4-byte store per entry, the
+    // cheapest for its accept branch), and the non-pressure pass, which walks every list
+    // first, regroups them into nbr_out (the same memory as nbr) with 16-byte stores.
     const int32_t* nbr;
     const int32_t* nbr_count;
+    const int32_t* nbr_src;
+    int32_t* nbr_out;
     // tables (5 x 1001) and colliders
     const float* tables;
     const Collider* colliders;

@@ -82,12 +82,11 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
         lo[a] = min(max(lo[a], o[a]), o[a] + d[a] - 1) - o[a];
         hi[a] = min(max(hi[a], o[a]), o[a] + d[a] - 1) - o[a];
     }
-    const int cap = P.nbr_cap;   // a multiple of 4: whole groups
+    const int cap = P.nbr_cap;
     const int64_t stride = P.nbr_stride;
-    // Accepted entries shift through `grp` (the newest in .w) and go out four at a time
-    // (list_entry's layout).
-    int4* out = reinterpret_cast<int4*>(nbr) + i;
-    int4 grp = make_int4(0, 0, 0, 0);
+    // Plain column-major (entry c at nbr[c * stride + i]); the non-pressure pass regroups the
+    // lists into list_entry's layout for the walks after it.
+    int32_t* out = nbr + i;
     int c = 0;
     if (lo[2] <= hi[2]) {
         for (int cx = lo[0]; cx <= hi[0]; cx++) {
@@ -103,11 +102,8 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
                     if (s <= P.h2) {
                         if (kDensity) sum += lookup_sq(W, TH2, s, P);
                         if (c < cap) {
-                            grp = make_int4(grp.y, grp.z, grp.w, q);
-                            if ((c & 3) == 3) {
-                                *out = grp;
-                                out += stride;
-                            }
+                            *out = q;
+                            out += stride;
                         }
                         c++;
                     }
@@ -115,12 +111,6 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
             }
         }
     }
-    // The last, partial group: its `rest` entries sit in the top components (its unused
-    // components are never read).
-    const int rest = c < cap ? (c & 3) : 0;
-    if (rest == 1) *out = make_int4(grp.w, 0, 0, 0);
-    if (rest == 2) *out = make_int4(grp.z, grp.w, 0, 0);
-    if (rest == 3) *out = make_int4(grp.y, grp.z, grp.w, 0);
     if (kDensity) *wsum = sum;
     return c;
 }
@@ -218,7 +208,7 @@ __device__ __forceinline__ void nonpressure_walk(const DevParams& P, const StepB
         float4 x, v;
         float rho;
     };
-    for_each_neighbor<2>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
+    for_each_neighbor_regroup(b.nbr_src, b.nbr_out, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return Rec{b.pos[j], b.vel[j], b.rho[j]}; },
                          [&](int j, const Rec& r) {
                              const V3 xj = v3(r.x);
