@@ -73,7 +73,8 @@ template <int T>
 __global__ void __launch_bounds__(T) kb_neighbors_density(BatchArgs a, const float4* __restrict__ pos,
                                                           const uint32_t* __restrict__ cell_start,
                                                           int32_t* __restrict__ nbr, int32_t* __restrict__ count,
-                                                          float* __restrict__ rho, float* __restrict__ pres)
+                                                          float* __restrict__ rho, float* __restrict__ pres,
+                                                          const float4* __restrict__ vel, float4* __restrict__ vrho)
 {
     __shared__ DevParams P;
     __shared__ float W[kTableSize], TH2[kTableSize + 1];
@@ -95,6 +96,8 @@ __global__ void __launch_bounds__(T) kb_neighbors_density(BatchArgs a, const flo
         if (pr < 0.f) pr *= P.neg;
         rho[i] = r;
         pres[i] = pr;
+        const float4 v = vel[i];
+        vrho[i] = make_float4(v.x, v.y, v.z, r);
         // Batch-wide, like the rest of the non-pressure pass's range checks (k_rank_gather).
         if (!exact_div_density(r)) atomicOr(&a.st[a.scenes].np_unsafe, 1u);
     }
@@ -427,11 +430,12 @@ int launch_batch_keys(const BatchArgs& a, const float4* pos, uint32_t* key, uint
 }
 
 int launch_batch_neighbors_density(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
-                                   int32_t* count, float* rho, float* pres, cudaStream_t s)
+                                   int32_t* count, float* rho, float* pres, const float4* vel, float4* vrho,
+                                   cudaStream_t s)
 {
     if (!a.items_count) return 0;
     LSP_BATCH_DISPATCH(a.threads, (kb_neighbors_density<T><<<a.items_count, T, 0, s>>>(a, pos, cell_start, nbr,
-                                                                                      count, rho, pres)));
+                                                                                      count, rho, pres, vel, vrho)));
     return 1;
 }
 

@@ -185,7 +185,7 @@ void BatchEngine::build()
         pos_[k].alloc(cap); vel_[k].alloc(cap); half_[k].alloc(cap); old_[k].alloc(cap);
     }
     force_.alloc(cap); ppos_.alloc(cap); ppos_alt_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
-    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap);
+    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap); vrho_.alloc(cap);
     key_.alloc(cap); slot_.alloc(cap); sorted_key_.alloc(cap); tmp_.alloc(cap);
     slot_of_id_.alloc(cap); nbr_count_.alloc(cap);
     // The scan reads and writes the histogram and cell table 8 entries at a time: both are
@@ -350,7 +350,7 @@ StepBuffers BatchEngine::buffers(int c)
     b.pos = pos_[c].p; b.vel = vel_[c].p; b.half = half_[c].p; b.old = old_[c].p;
     b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
-    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p;
+    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p; b.vrho = vrho_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p + sc_.size();
     b.hist = history_on() ? phist_[c].p : nullptr;
     b.gradrho = features_on() ? gradrho_.p : nullptr;
@@ -382,7 +382,7 @@ int BatchEngine::enqueue_step(int c, int grid)
     launches += launch_grid_order(g, stream_);
     StepBuffers b = buffers(1 - c);
     launches += launch_batch_neighbors_density(a, pos_[1 - c].p, cell_start_.p, nbr_src_.p, nbr_count_.p, rho_.p,
-                                               pres_.p, stream_);
+                                               pres_.p, vel_[1 - c].p, vrho_.p, stream_);
     launches += launch_batch_nonpressure(a, b, stream_);
     if (pcisph_) {
         CK(cudaMemsetAsync(loop_sync_.p, 0, 4 * sizeof(uint32_t), stream_));

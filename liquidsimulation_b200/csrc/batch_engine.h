@@ -115,6 +115,7 @@ private:
     DevArray<float4> pos_[2], vel_[2], half_[2], old_[2];
     DevArray<float4> force_, ppos_, ppos_alt_, phalf_, pforce_;
     DevArray<float> rho_, pres_, prho_, err_;
+    DevArray<float4> vrho_;   // {v, rho} for the non-pressure pass (StepBuffers::vrho)
     DevArray<uint32_t> key_, slot_, sorted_key_, hist_, cell_start_, tile_sums_, loop_sync_, maxerr_;
     DevArray<int2> tmp_;
     DevArray<int32_t> slot_of_id_, nbr_, nbr_src_, nbr_count_;   // nbr_: grouped lists; nbr_src_: the build's plain lists

@@ -46,7 +46,8 @@ int launch_batch_keys(const BatchArgs& a, const float4* pos, uint32_t* key, uint
                       cudaStream_t s);
 // Lists plus the start-of-step density and pressure (rho, pres), per item.
 int launch_batch_neighbors_density(const BatchArgs& a, const float4* pos, const uint32_t* cell_start, int32_t* nbr,
-                                   int32_t* count, float* rho, float* pres, cudaStream_t s);
+                                   int32_t* count, float* rho, float* pres, const float4* vel, float4* vrho,
+                                   cudaStream_t s);
 int launch_batch_nonpressure(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
 int launch_batch_sph_pressure(const BatchArgs& a, const StepBuffers& b, cudaStream_t s);
 int launch_batch_integrate(const BatchArgs& a, const StepBuffers& b, bool add_pforce, cudaStream_t s);

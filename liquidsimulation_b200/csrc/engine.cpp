@@ -267,7 +267,7 @@ void Engine::ensure_capacity(int64_t n)
     pos_[1 - cur_].alloc(cap); vel_[1 - cur_].alloc(cap); half_[1 - cur_].alloc(cap); old_[1 - cur_].alloc(cap);
     force_.alloc(cap); ppos_.alloc(cap); ppos_alt_.alloc(cap); phalf_.alloc(cap); pforce_.alloc(cap);
     ppos_final_ = ppos_.p;
-    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap);
+    rho_.alloc(cap); pres_.alloc(cap); prho_.alloc(cap); err_.alloc(cap); vrho_.alloc(cap);
     key_.alloc(cap); slot_.alloc(cap); sorted_key_.alloc(cap); tmp_.alloc(cap); nbr_count_.alloc(cap);
     stage_.alloc(cap * 12);
     CK(cudaMemsetAsync(force_.p, 0, cap * sizeof(float4), stream_));
@@ -506,7 +506,7 @@ StepBuffers Engine::buffers()
     b.pos = pos_[cur_].p; b.vel = vel_[cur_].p; b.half = half_[cur_].p; b.old = old_[cur_].p;
     b.force = force_.p; b.rho = rho_.p; b.pres = pres_.p;
     b.ppos = ppos_.p; b.phalf = phalf_.p; b.pforce = pforce_.p; b.prho = prho_.p; b.err = err_.p;
-    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p;
+    b.nbr = nbr_.p; b.nbr_count = nbr_count_.p; b.nbr_src = nbr_src_.p; b.nbr_out = nbr_.p; b.vrho = vrho_.p;
     b.tables = tables_.p; b.colliders = dcols_.p; b.status = status_.p;
     b.hist = phist_[cur_].p;
     b.gradrho = features_on() ? gradrho_.p : nullptr;
@@ -770,7 +770,7 @@ void Engine::run_step(float dt, lsp_step_stats* st)
         g.hist_in = phist_[cur_].p; g.hist_out = phist_[1 - cur_].p;
         g.nbr = nbr_src_.p; g.nbr_count = nbr_count_.p; g.status = status_.p;
         // The neighbour build also sums the start-of-step density (k_neighbors_density).
-        g.tables = tables_.p; g.rho = rho_.p; g.pres = pres_.p;
+        g.tables = tables_.p; g.rho = rho_.p; g.pres = pres_.p; g.vrho = vrho_.p;
         timed(LSP_PROF_GRID_SORT, [&] { return launch_grid_keys(g, stream_); });
         timed(LSP_PROF_GRID_SCAN, [&] { return launch_grid_scan(g, stream_); });
         timed(LSP_PROF_GRID_SCATTER, [&] { return launch_grid_scatter(g, stream_); });

@@ -152,6 +152,7 @@ private:
     const float4* ppos_final_ = nullptr;   // buffer holding the last iteration's x*
     DevArray<uint32_t> loop_sync_, maxerr_;
     DevArray<float> rho_, pres_, prho_, err_;
+    DevArray<float4> vrho_;   // {v, rho} for the non-pressure pass (StepBuffers::vrho)
     DevArray<uint32_t> key_, slot_, sorted_key_;
     DevArray<int2> tmp_;
     DevArray<int32_t> slot_of_id_, nbr_, nbr_src_, nbr_count_;   // nbr_: grouped lists; nbr_src_: the build's plain lists

@@ -218,7 +218,8 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
 __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
                                     const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
                                     int32_t* __restrict__ count, DevStatus* st, const float* __restrict__ tables,
-                                    float* __restrict__ rho, float* __restrict__ pres)
+                                    float* __restrict__ rho, float* __restrict__ pres,
+                                    const float4* __restrict__ vel, float4* __restrict__ vrho)
 {
     __shared__ float W[kTableSize], TH2[kTableSize + 1];
     stage_table(W, tables, T_W);
@@ -236,6 +237,8 @@ __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
         if (pr < 0.f) pr *= P.neg;
         rho[i] = r;
         pres[i] = pr;
+        const float4 v = vel[i];
+        vrho[i] = make_float4(v.x, v.y, v.z, r);
         if (!exact_div_density(r)) atomicOr(&st->np_unsafe, 1u);
     }
     record_neighbor_count(P, c, valid, st);
@@ -313,7 +316,7 @@ int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)
     const int T = 256;
     if (a.P.n <= 0) return 0;
     k_neighbors_density<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
-                                                           a.status, a.tables, a.rho, a.pres);
+                                                           a.status, a.tables, a.rho, a.pres, a.vel_out, a.vrho);
     return 1;
 }
 

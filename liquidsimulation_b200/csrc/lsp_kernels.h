@@ -36,6 +36,7 @@ struct GridBuildArgs {
     const float* tables;
     float* rho;
     float* pres;
+    float4* vrho;          // {v, rho} per particle for the non-pressure pass's gathers
 };
 
 struct MlpPacked;
@@ -75,6 +76,9 @@ struct StepBuffers {
     const int32_t* nbr_count;
     const int32_t* nbr_src;
     int32_t* nbr_out;
+    // {v.x, v.y, v.z, rho} of each particle, written by the neighbour build once rho is known:
+    // the non-pressure pass gathers a neighbour's velocity and density with one 16-byte load.
+    const float4* vrho;
     // tables (5 x 1001) and colliders
     const float* tables;
     const Collider* colliders;

@@ -205,11 +205,10 @@ __device__ __forceinline__ void nonpressure_walk(const DevParams& P, const StepB
     float lap = 0.f;
     V3 grad = v3(0.f, 0.f, 0.f);   // sum (rho_j - rho_i) / rho_j grad W_ij: a warm-start feature only
     struct Rec {
-        float4 x, v;
-        float rho;
+        float4 x, vr;   // position; velocity and density ({v, rho}, StepBuffers::vrho)
     };
     for_each_neighbor_regroup(b.nbr_src, b.nbr_out, i, P.nbr_stride, __ldg(b.nbr_count + i),
-                         [&](int j) { return Rec{b.pos[j], b.vel[j], b.rho[j]}; },
+                         [&](int j) { return Rec{b.pos[j], b.vrho[j]}; },
                          [&](int j, const Rec& r) {
                              const V3 xj = v3(r.x);
                              V3 dir = xi - xj;
@@ -217,21 +216,21 @@ __device__ __forceinline__ void nonpressure_walk(const DevParams& P, const StepB
                              const NonpressureWeights at(NA, NB, sqmag(dir), P);
                              const float w_dw = at.dw;
                              if (kExactDiv) {
-                                 const float y = recip_rn(r.rho);
-                                 auto q = [&](float a) { return div_by(a, r.rho, y); };
+                                 const float y = recip_rn(r.vr.w);
+                                 auto q = [&](float a) { return div_by(a, r.vr.w, y); };
                                  const V3 n = dir * w_dw;
                                  normal += v3(q(n.x), q(n.y), q(n.z));
                                  lap += q(at.d2w);
                                  if (j != i) {
-                                     const V3 dv = v3(r.v) - vi;
+                                     const V3 dv = v3(r.vr) - vi;
                                      visc += v3(q(dv.x), q(dv.y), q(dv.z)) * at.vd2w;
                                  }
-                                 if (kGrad) grad += dir * (w_dw * q(r.rho - rhoi));
+                                 if (kGrad) grad += dir * (w_dw * q(r.vr.w - rhoi));
                              } else {
-                                 normal += dir * w_dw / r.rho;
-                                 lap += at.d2w / r.rho;
-                                 if (j != i) visc += ((v3(r.v) - vi) / r.rho) * at.vd2w;
-                                 if (kGrad) grad += dir * (w_dw * ((r.rho - rhoi) / r.rho));
+                                 normal += dir * w_dw / r.vr.w;
+                                 lap += at.d2w / r.vr.w;
+                                 if (j != i) visc += ((v3(r.vr) - vi) / r.vr.w) * at.vd2w;
+                                 if (kGrad) grad += dir * (w_dw * ((r.vr.w - rhoi) / r.vr.w));
                              }
                          });
     if (kGrad) b.gradrho[i] = P.mass * mag(grad);
