@@ -65,6 +65,9 @@ def test_library_arm_line():
     assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-3 and r["traffic"] > 0
     e = d["e2e"]
     assert e["value"] > 0 and e["h2d_bytes_per_step"] > 0 and e["d2h_bytes_per_step"] > 0
+    # The end-to-end arm replays the timed steps from their start state and arrives at the
+    # same bits as the timed steps.
+    assert e["replay_bit_identical"] is True
     assert d["gpu_launches"] > 0
     c = d["clocks"]
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(c) and c["samples"] > 0
