@@ -86,6 +86,9 @@ void HostKernels::build(const lsp_params& p)
     for (int k = 1; k <= sub; k++) thr2[k] = sq_bound(thr[k]);
     thr2[kTableSize] = std::numeric_limits<float>::infinity();
     cut2 = sq_bound(h);
+    uint32_t w_last;
+    std::memcpy(&w_last, &tables[0 * kTableSize + sub], 4);   // W at slot 1000
+    density_tail0 = w_last == 0u && thr2[sub] <= cut2;
     float stepSize = 1.6f * p.particle_radius;
     float sum = 0.f;
     for (int i = -3; i <= 3; i++)
@@ -484,6 +487,7 @@ DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt)
     P.min_it = p.pci_min_iterations;
     P.max_it = p.pci_max_iterations;
     P.exact_tables = hk.exact_tables ? 1 : 0;
+    P.density_tail0 = hk.density_tail0 ? 1 : 0;
     return P;
 }
 

@@ -25,6 +25,10 @@ struct HostKernels {
     // Laplacian) is 0 or within [2^-29, 2^60]: the pass may then divide by the neighbour
     // density with div_by (DevParams::exact_tables).
     bool exact_tables = false;
+    // The W table's last entry (slot 1000) is +0 and every s >= cut2 takes that slot
+    // (thr2[1000] <= cut2): the density lookups may then skip the cutoff's select
+    // (DevParams::density_tail0), since the slot already gives the cutoff's 0.
+    bool density_tail0 = false;
     void build(const lsp_params& p);
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;

@@ -215,6 +215,7 @@ __global__ void k_rank_gather(DevParams P, const int2* __restrict__ tmp, const u
 // its position gathers would cost more. (A list that
 // overflows its capacity raises the overflow flag and the step is redone, so the sum over
 // every accepted pair never differs from the stored list's.)
+template <bool kTail0>
 __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
                                     const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
                                     int32_t* __restrict__ count, DevStatus* st, const float* __restrict__ tables,
@@ -230,7 +231,7 @@ __global__ void k_neighbors_density(DevParams P, const float4* __restrict__ pos,
     int c = 0;
     if (valid) {
         float sum;
-        c = neighbors_one<true>(P, pos, cell_start, nbr, i, W, TH2, &sum);
+        c = neighbors_one<true, kTail0>(P, pos, cell_start, nbr, i, W, TH2, &sum);
         count[i] = min(c, P.nbr_cap);
         const float r = P.mass * sum;
         float pr = P.stiffness * (r - P.rho0);
@@ -315,8 +316,14 @@ int launch_neighbors(const GridBuildArgs& a, cudaStream_t s)
 {
     const int T = 256;
     if (a.P.n <= 0) return 0;
-    k_neighbors_density<<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
-                                                           a.status, a.tables, a.rho, a.pres, a.vel_out, a.vrho);
+    if (a.P.density_tail0)
+        k_neighbors_density<true><<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr, a.nbr_count,
+                                                                     a.status, a.tables, a.rho, a.pres, a.vel_out,
+                                                                     a.vrho);
+    else
+        k_neighbors_density<false><<<blocks_for(a.P.n, T), T, 0, s>>>(a.P, a.pos_out, a.cell_start, a.nbr,
+                                                                      a.nbr_count, a.status, a.tables, a.rho, a.pres,
+                                                                      a.vel_out, a.vrho);
     return 1;
 }
 

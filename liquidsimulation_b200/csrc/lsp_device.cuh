@@ -93,6 +93,7 @@ struct DevParams {
     int coll_off;
     int scene;
     int exact_tables;   // HostKernels::exact_tables
+    int density_tail0;  // HostKernels::density_tail0
 };
 
 // ----------------------------------------------------------------- vector ops
@@ -226,10 +227,13 @@ __device__ __forceinline__ float lookup(const float* tab, const float* thr, floa
 }
 // lookup(tab, thr, sqrt(s), P) bit for bit, from the squared distance (d >= h exactly when
 // s >= cut2).
+// kTail0 (DevParams::density_tail0, for the W table): every s >= cut2 takes slot 1000,
+// whose entry is +0, so the cutoff's select is redundant and left out.
+template <bool kTail0 = false>
 __device__ __forceinline__ float lookup_sq(const float* tab, const float* thr2, float s, const DevParams& P)
 {
     const float w = tab[table_slot_sq(s, P.inv_step, thr2)];
-    return (s >= P.cut2) ? 0.f : w;
+    return (kTail0 || !(s >= P.cut2)) ? w : 0.f;
 }
 
 // The non-pressure pass reads three tables at one squared distance s. Its slot records

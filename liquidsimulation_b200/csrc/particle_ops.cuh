@@ -61,7 +61,7 @@ __device__ __forceinline__ uint32_t cell_key(const DevParams& P, const float4& p
 // returns the true count. With kDensity it also sums W over the accepted pairs in list
 // order from their squared distances, the sum density_one forms over the stored list
 // (|x_i - x_j|^2 equals |x_j - x_i|^2 bit for bit; W and TH2 as in density_one).
-template <bool kDensity = false>
+template <bool kDensity = false, bool kTail0 = false>
 __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* __restrict__ pos,
                                              const uint32_t* __restrict__ cell_start, int32_t* __restrict__ nbr,
                                              int i, const float* W = nullptr, const float* TH2 = nullptr,
@@ -100,7 +100,7 @@ __device__ __forceinline__ int neighbors_one(const DevParams& P, const float4* _
                     const V3 dq = xi - v3(*pq);
                     const float s = sqmag(dq);
                     if (s <= P.h2) {
-                        if (kDensity) sum += lookup_sq(W, TH2, s, P);
+                        if (kDensity) sum += lookup_sq<kTail0>(W, TH2, s, P);
                         if (c < cap) {
                             *out = q;
                             out += stride;
@@ -341,7 +341,8 @@ __device__ __forceinline__ void pci_predict_one(const DevParams& P, const StepBu
 
 // PCISPHSolver.cpp:100-126 for one particle; returns |error| (0 for NaN, which the
 // reference's std::max ignores). Table lookups on the squared distance (TH2), as in
-// density_one.
+// density_one (kTail0: DevParams::density_tail0 holds).
+template <bool kTail0 = false>
 __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepBuffers& b, const float* W,
                                                  const float* TH2, int i, int iteration, float4* ppos)
 {
@@ -349,7 +350,7 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
     float sum = 0.f;
     for_each_neighbor<4>(b.nbr, i, P.nbr_stride, __ldg(b.nbr_count + i),
                          [&](int j) { return ppos[j]; },
-                         [&](int, float4 pj) { sum += lookup_sq(W, TH2, sqmag(v3(pj) - xi), P); });
+                         [&](int, float4 pj) { sum += lookup_sq<kTail0>(W, TH2, sqmag(v3(pj) - xi), P); });
     float pd = P.mass * sum;
     float er = pd - P.rho0;
     float pp = P.delta * er;

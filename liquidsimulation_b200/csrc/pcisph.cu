@@ -134,6 +134,7 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 // slower too), and one block of 1024 beats two of 512 by 3.5 % and four of 256 by 4 % (a
 // grid barrier with 148 arrivals, one table copy per SM).
 constexpr int kLoopThreads = 1024;
+template <bool kTail0>   // DevParams::density_tail0
 __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt,
                                                              LoopSync* sy, uint32_t* maxerr, int first_done, int warm)
 {
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     // density(k) over all particles; the block maximum of |error| goes to maxerr[slot].
     auto density_pass = [&](int k, int slot) {
         float m = 0.f;
-        for_particles([&](int i) { m = fmaxf(m, pci_density_one(P, b, W, TH2, i, k, pp(k & 1))); });
+        for_particles([&](int i) { m = fmaxf(m, pci_density_one<kTail0>(P, b, W, TH2, i, k, pp(k & 1))); });
         uint32_t mb = __float_as_uint(m);
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) mb = max(mb, __shfl_xor_sync(0xffffffffu, mb, off));
@@ -236,12 +237,12 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
     }
 }
 
-// Per device and block size (1024 / 512 / 256 / 128 threads): resident blocks of k_pci_loop
-// per SM (0: no cooperative launch).
+// Per device, instance (kTail0) and block size (1024 / 512 / 256 / 128 threads): resident
+// blocks of k_pci_loop per SM (0: no cooperative launch).
 constexpr int kMaxDevices = 64;
 constexpr int kLoopShapes = 4;
 // Filled once per device under a lock (solvers on different host threads may launch at once).
-static int g_loop_blocks_per_sm[kMaxDevices][kLoopShapes];
+static int g_loop_blocks_per_sm[kMaxDevices][2][kLoopShapes];
 static bool g_loop_ready[kMaxDevices];
 static std::mutex g_loop_mutex;
 
@@ -266,19 +267,22 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     if (!g_loop_ready[dev]) {
         int coop = 0;
         cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev);
-        for (int k = 0; k < kLoopShapes; k++) {
-            int per = 0;
-            if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pci_loop, kLoopThreads >> k, 0) !=
-                             cudaSuccess)
-                per = 0;
-            g_loop_blocks_per_sm[dev][k] = per;
-        }
+        for (int t = 0; t < 2; t++)
+            for (int k = 0; k < kLoopShapes; k++) {
+                int per = 0;
+                const void* fn = t ? (const void*)k_pci_loop<true> : (const void*)k_pci_loop<false>;
+                if (!coop || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kLoopThreads >> k, 0) !=
+                                 cudaSuccess)
+                    per = 0;
+                g_loop_blocks_per_sm[dev][t][k] = per;
+            }
         g_loop_ready[dev] = true;
     }
     const int sms = device_sm_count();
     const int shape = loop_shape(P.n, sms);
     const int threads = kLoopThreads >> shape;
-    const int per_sm = g_loop_blocks_per_sm[dev][shape];
+    const int tail0 = P.density_tail0 ? 1 : 0;
+    const int per_sm = g_loop_blocks_per_sm[dev][tail0][shape];
     lock.unlock();
     if (per_sm <= 0) return false;
     int need = (int)((P.n + threads - 1) / threads);
@@ -287,7 +291,8 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     StepBuffers bc = b;
     LoopSync* sy = (LoopSync*)sync;
     void* args[] = {&Pc, &bc, &ppos_alt, &sy, &maxerr, &first_done, &warm};
-    if (cudaLaunchCooperativeKernel((const void*)k_pci_loop, dim3(grid), dim3(threads), args, 0, s) != cudaSuccess)
+    const void* fn = tail0 ? (const void*)k_pci_loop<true> : (const void*)k_pci_loop<false>;
+    if (cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(threads), args, 0, s) != cudaSuccess)
         return false;
     if (grid_used) *grid_used = grid;
     return true;
