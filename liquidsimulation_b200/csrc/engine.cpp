@@ -89,6 +89,9 @@ void HostKernels::build(const lsp_params& p)
     uint32_t w_last;
     std::memcpy(&w_last, &tables[0 * kTableSize + sub], 4);   // W at slot 1000
     density_tail0 = w_last == 0u && thr2[sub] <= cut2;
+    uint32_t sdw_last;
+    std::memcpy(&sdw_last, &tables[3 * kTableSize + sub], 4);   // spiky gradient at slot 1000
+    force_tail0 = (sdw_last & 0x7fffffffu) == 0u && thr[sub] <= h;
     float stepSize = 1.6f * p.particle_radius;
     float sum = 0.f;
     for (int i = -3; i <= 3; i++)
@@ -488,6 +491,7 @@ DevParams physics_params(const lsp_params& p, const HostKernels& hk, float dt)
     P.max_it = p.pci_max_iterations;
     P.exact_tables = hk.exact_tables ? 1 : 0;
     P.density_tail0 = hk.density_tail0 ? 1 : 0;
+    P.force_tail0 = hk.force_tail0 ? 1 : 0;
     return P;
 }
 

@@ -29,6 +29,9 @@ struct HostKernels {
     // (thr2[1000] <= cut2): the density lookups may then skip the cutoff's select
     // (DevParams::density_tail0), since the slot already gives the cutoff's 0.
     bool density_tail0 = false;
+    // The same for the spiky gradient table and the distance cutoff: its last entry is a zero
+    // and every d >= h takes slot 1000 (thr[1000] <= h) (DevParams::force_tail0).
+    bool force_tail0 = false;
     void build(const lsp_params& p);
     float delta(const lsp_params& p, float dt) const;
     float look(int t, float d) const;

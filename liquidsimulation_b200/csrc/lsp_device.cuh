@@ -94,6 +94,7 @@ struct DevParams {
     int scene;
     int exact_tables;   // HostKernels::exact_tables
     int density_tail0;  // HostKernels::density_tail0
+    int force_tail0;    // HostKernels::force_tail0
 };
 
 // ----------------------------------------------------------------- vector ops
@@ -220,10 +221,15 @@ __device__ __forceinline__ int table_slot_sq(float s, float inv_step, const floa
 
 // The table read is unconditional (the slot is always inside the table) and the cutoff a
 // select: measured faster than branching around the read.
+// kTail0 (DevParams::force_tail0, for the spiky table): every d >= h takes slot 1000, whose
+// entry is a zero, so the cutoff's select is left out. (Its sign may be negative; a force sum
+// starts at +0 and a sum of roundings to nearest never reaches -0 from there, so adding either
+// zero leaves it unchanged.)
+template <bool kTail0 = false>
 __device__ __forceinline__ float lookup(const float* tab, const float* thr, float d, const DevParams& P)
 {
     const float w = tab[table_slot(d, P.inv_step, thr)];
-    return (d >= P.h) ? 0.f : w;
+    return (kTail0 || !(d >= P.h)) ? w : 0.f;
 }
 // lookup(tab, thr, sqrt(s), P) bit for bit, from the squared distance (d >= h exactly when
 // s >= cut2).

@@ -376,7 +376,7 @@ __device__ __forceinline__ float pci_density_one(const DevParams& P, const StepB
 // with kExactDiv they come from sqrt_rn and one reciprocal of d (recip_rn, div_by), the same
 // bits for the predicted positions the step's predict passes found safe
 // (DevStatus::div_unsafe clear).
-template <bool kExactDiv>
+template <bool kExactDiv, bool kTail0 = false>
 __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuffers& b, const float* SDW,
                                                const float* TH, int i, const float4* ppos)
 {
@@ -399,17 +399,18 @@ __device__ __forceinline__ void pci_force_walk(const DevParams& P, const StepBuf
                              } else {
                                  dir = dq / d;
                              }
-                             pf += dir * lookup(SDW, TH, d, P) * (tf + pj4.w);
+                             pf += dir * lookup<kTail0>(SDW, TH, d, P) * (tf + pj4.w);
                          });
     pf *= -(P.mass * b.rho[i]);
     if (isnan(pf.x)) pf = v3(0.f, 0.f, 0.f);
     b.pforce[i] = f4(pf, 0.f);
 }
+template <bool kTail0 = false>
 __device__ __forceinline__ void pci_force_one(const DevParams& P, const StepBuffers& b, const float* SDW,
                                               const float* TH, int i, const float4* ppos)
 {
-    if (*(const volatile uint32_t*)&b.status->div_unsafe == 0u) pci_force_walk<true>(P, b, SDW, TH, i, ppos);
-    else pci_force_walk<false>(P, b, SDW, TH, i, ppos);
+    if (*(const volatile uint32_t*)&b.status->div_unsafe == 0u) pci_force_walk<true, kTail0>(P, b, SDW, TH, i, ppos);
+    else pci_force_walk<false, kTail0>(P, b, SDW, TH, i, ppos);
 }
 
 }  // namespace lsp

@@ -134,7 +134,7 @@ void launch_pci_density_first(const DevParams& P, const StepBuffers& b, const Wa
 // slower too), and one block of 1024 beats two of 512 by 3.5 % and four of 256 by 4 % (a
 // grid barrier with 148 arrivals, one table copy per SM).
 constexpr int kLoopThreads = 1024;
-template <bool kTail0>   // DevParams::density_tail0
+template <bool kTail0>   // DevParams::density_tail0 && DevParams::force_tail0
 __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepBuffers b, float4* ppos_alt,
                                                              LoopSync* sy, uint32_t* maxerr, int first_done, int warm)
 {
@@ -213,7 +213,7 @@ __global__ void __launch_bounds__(kLoopThreads, 1) k_pci_loop(DevParams P, StepB
         const bool unverified = warm && !rejected && k == 0;
         const bool done = (conv && k + 1 >= P.min_it && !unverified) || (k + 1 >= P.max_it);
         for_particles([&](int i) {
-            pci_force_one(P, b, SDW, TH, i, pp(k & 1));
+            pci_force_one<kTail0>(P, b, SDW, TH, i, pp(k & 1));
             // The last pass also integrates and collides the particle (SPHParticle::integrate
             // after the loop, PCISPHSolver.cpp:166-169): it reads only the particle's own
             // state and pressure force, which this thread has just written, and no thread of
@@ -281,7 +281,7 @@ bool launch_pci_loop(const DevParams& P, const StepBuffers& b, float4* ppos_alt,
     const int sms = device_sm_count();
     const int shape = loop_shape(P.n, sms);
     const int threads = kLoopThreads >> shape;
-    const int tail0 = P.density_tail0 ? 1 : 0;
+    const int tail0 = (P.density_tail0 && P.force_tail0) ? 1 : 0;
     const int per_sm = g_loop_blocks_per_sm[dev][tail0][shape];
     lock.unlock();
     if (per_sm <= 0) return false;
