@@ -364,10 +364,10 @@ __device__ __forceinline__ int list_entry(const int32_t* __restrict__ nbr, int64
 }
 
 // for_each_neighbor (B = 2) over particle i's plain column-major list `src` (entry k at
-// src[k * stride + i]) that also stores the list in list_entry's grouped layout at `dst`: each
-// pair of entries goes out as one 8-byte store (half a group; all lanes store in step, so the
-// stores coalesce), and the next pair's indices are in flight while the current pair's records
-// are fetched and its pairs computed, as in for_each_neighbor.
+// src[k * stride + i]) that also stores the list in list_entry's grouped layout at `dst`: every
+// second pair of entries completes a group, which goes out as one 16-byte store (all lanes store
+// in step, so the stores coalesce), and the next pair's indices are in flight while the current
+// pair's records are fetched and its pairs computed, as in for_each_neighbor.
 template <typename Load, typename F>
 __device__ __forceinline__ void for_each_neighbor_regroup(const int32_t* __restrict__ src, int32_t* __restrict__ dst,
                                                           int i, int64_t stride, int cnt, Load load, F f)
@@ -381,6 +381,7 @@ __device__ __forceinline__ void for_each_neighbor_regroup(const int32_t* __restr
         j1 = __ldg(l + stride);
         l += 2 * stride;
     }
+    int p0 = 0, p1 = 0;   // the first pair of the current group
     for (int b = 0; b < full; b++) {
         const auto r0 = load(j0);
         const auto r1 = load(j1);
@@ -390,17 +391,26 @@ __device__ __forceinline__ void for_each_neighbor_regroup(const int32_t* __restr
             n1 = __ldg(l + stride);
             l += 2 * stride;
         }
-        reinterpret_cast<int2*>(g)[b & 1] = make_int2(j0, j1);
-        if (b & 1) g += 4 * stride;
+        if (b & 1) {
+            *reinterpret_cast<int4*>(g) = make_int4(p0, p1, j0, j1);
+            g += 4 * stride;
+        } else {
+            p0 = j0;
+            p1 = j1;
+        }
         f(j0, r0);
         f(j1, r1);
         j0 = n0;
         j1 = n1;
     }
+    // The last, partial group: a pending pair and / or the odd last entry (its unused
+    // components are never read).
     if (cnt & 1) {
         const int jj = __ldg(l);
-        g[2 * (full & 1)] = jj;
+        *reinterpret_cast<int4*>(g) = (full & 1) ? make_int4(p0, p1, jj, 0) : make_int4(jj, 0, 0, 0);
         f(jj, load(jj));
+    } else if (full & 1) {
+        *reinterpret_cast<int4*>(g) = make_int4(p0, p1, 0, 0);
     }
 }
 
