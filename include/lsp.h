@@ -183,7 +183,9 @@ int lsp_read_state(lsp_solver* s, float* x, float* v, float* half, float* old_ha
 int lsp_write_state(lsp_solver* s, const float* x, const float* v, const float* half, const float* old_half, const int32_t* first, int64_t n);
 
 /* Start-of-step neighbour lists of the last step, caller order, in the reference's
- * order (SPHSpatialGrid::findNeighborParticles, SPHSpatialGrid.cpp:39-76).
+ * order (SPHSpatialGrid::findNeighborParticles, SPHSpatialGrid.cpp:39-76). Like the grid
+ * read-back and lsp_mlp_train, refused with LSP_ERR_STATE until a step has run on the current
+ * particles (after lsp_add_particles or lsp_remove_particles, until the next step).
  * offsets: int64[n+1]; index: int32[offsets[n]] (pass index=NULL to get offsets only). */
 int lsp_read_neighbors(lsp_solver* s, int64_t* offsets, int32_t* index, int64_t n, int64_t capacity);
 

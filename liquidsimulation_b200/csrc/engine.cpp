@@ -325,12 +325,14 @@ void Engine::add_particles(const float* xyz, const float* vel, int64_t m)
     CK(cudaStreamSynchronize(stream_));
     n_ += m;
     if (domain_from_particles_) grid_valid_ = false;
+    stepped_ = false;   // the last step's lists, grid and features no longer cover every particle
 }
 
 void Engine::remove_particles()
 {
     n_ = 0;
     if (domain_from_particles_) grid_valid_ = false;
+    stepped_ = false;
 }
 
 int Engine::add_collider(const Collider& c)
@@ -1059,7 +1061,6 @@ void Engine::mlp_record(bool on)
     if (on) ensure_warm_buffers();
 }
 
-// Adam steps on the features and final pressures of the last step (targets p / p_scale).
 // Adam steps on the features and final pressures of the last step (targets p / p_scale).
 float Engine::mlp_train(int iterations, int batch, float lr, uint64_t seed)
 {

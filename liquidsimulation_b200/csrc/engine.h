@@ -195,7 +195,7 @@ private:
     int64_t prof_n_[LSP_PROF_COUNT] = {};
     int64_t launches_ = 0;
     DevArray<int32_t> bounds_;
-    bool stepped_ = false;
+    bool stepped_ = false;   // a step has run on the current particle set (lists, grid, features valid)
 
     // Learned warm start state.
     bool features_on() const;

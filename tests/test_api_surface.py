@@ -8,6 +8,9 @@
 - Read-back (SPHSolver.cpp:384-429): lsp_read_particles gives the position and velocity
   fields in caller order; the batch's counts, masses and read-back agree with its scenes.
 - lsp_device_info reports the device the library runs on.
+- The products of a step (neighbour lists, grid, recorded features) describe the particles of
+  that step: after particles are added or removed they are refused (LSP_ERR_STATE) until the
+  next step.
 """
 import ctypes
 
@@ -153,3 +156,29 @@ def test_device_info():
     props = torch.cuda.get_device_properties(0)
     assert (sms.value, major.value, minor.value) == (props.multi_processor_count, props.major, props.minor)
     assert major.value == 10
+
+
+def test_step_products_need_a_step_on_the_current_particles():
+    sc = scenes.small_box_scene(n_side=(6, 6, 6), seed=10)
+    gpu = from_scene(sc)
+    try:
+        gpu.mlp_record(True)
+        gpu.update(sc.dt)
+        gpu.neighbors()
+        gpu.grid()
+        extra = scenes.lattice((0.5, 0.5, 0.5), (3, 3, 3), 0.02, 11)
+        gpu.add_particles(extra)
+        for call in (gpu.neighbors, gpu.grid, lambda: gpu.mlp_train(iterations=1, batch=64)):
+            with pytest.raises(abi.LspError) as e:
+                call()
+            assert e.value.code == abi.LSP_ERR_STATE
+        gpu.update(sc.dt)
+        off, idx = gpu.neighbors()
+        assert off.size == sc.n + extra.shape[0] + 1 and idx.size == off[-1]
+        gpu.mlp_train(iterations=1, batch=64)
+        gpu.remove_particles()
+        with pytest.raises(abi.LspError) as e:
+            gpu.neighbors()
+        assert e.value.code == abi.LSP_ERR_STATE
+    finally:
+        gpu.close()
