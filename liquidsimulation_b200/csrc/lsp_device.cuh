@@ -356,8 +356,9 @@ __device__ __forceinline__ void collide_all(const Collider* cols, int ncoll, V3&
 // Neighbour-list layout: entry k of particle i is component k & 3 of the int4 at group k >> 2,
 // and each group is column-major over the particles (group g of particle i at
 // ((int4*)nbr)[g * stride + i]). A reader fetches four indices with one coalesced 16-byte
-// load; the builder writes four entries with one store instead of four scattered 4-byte
-// ones (each a separate L2 request: the list build is bound by their rate).
+// load. The neighbour build writes plain column-major lists (one 4-byte store per accepted
+// entry, the cheapest for its accept branch) and the non-pressure pass, which walks every
+// list first, stores them in this layout (for_each_neighbor_regroup).
 __device__ __forceinline__ int list_entry(const int32_t* __restrict__ nbr, int64_t stride, int64_t i, int k)
 {
     return nbr[(((int64_t)(k >> 2) * stride + i) << 2) + (k & 3)];
